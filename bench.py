@@ -1,0 +1,398 @@
+"""Benchmark of the finite-difference hot path on B200.
+
+Workload (one GPU): the 3D operator sweep on a 512^3 float32 grid — a scalar
+field and a 3-component vector field, standard normal values (seeded), ghost
+width 1 for order 2 and 2 for order 4, periodic ghosts filled once before
+timing.  One step applies, for each order (2 and 4): Laplacian(scalar),
+Grad(scalar -> vec3) and Divergence(vec3 -> scalar), i.e. 6 operator
+applications over the 512^3 interior.  Metric: cell-updates/s (interior cells
+x operator applications / s).  Every input is larger than L2 (126 MB), so no
+L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--gpus N > 1 (under torchrun): weak scaling, each rank owns one 512^3 slab of
+an (N*512) x 512 x 512 periodic domain; its X ghost planes come from the
+neighbouring ranks once before timing (NCCL send/recv), so the timed steps
+have no collective.  --impl reference times the CPU restatement of the
+reference's operators (oracle/fdm.py, float32, reference operation order) on
+the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_INT = 512
+METRIC = "cell-updates/s (3D operator sweep: Laplacian, Grad, Divergence; order 2 and 4)"
+UNIT = "cell-updates/s"
+# algorithmic bytes per interior cell: compulsory read once + write once
+ALG_BYTES = {"laplacian": 8, "grad": 16, "divergence": 16}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ------------------------------------------------------------ clocks ---
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------- CPU baseline ---
+def cpu_sweep_sample(n: int, threads: int, reps: int = 1):
+    """Time the float32 oracle over the 6-operator step on an n^3 interior,
+    split into X slabs over `threads` threads (NumPy releases the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import fdm
+    rng = np.random.default_rng(1)
+    dx = 1.0 / N_INT
+    fields = {}
+    for order in (2, 4):
+        g = order // 2
+        s = n + 2 * g
+        fields[order] = (rng.standard_normal((s, s, s, 1), dtype=np.float32),
+                         rng.standard_normal((s, s, s, 3), dtype=np.float32))
+
+    def slab_job(order, x0, x1):
+        g = order // 2
+        u, v = fields[order]
+        us, vs = u[x0 - g:x1 + g], v[x0 - g:x1 + g]
+        fdm.laplacian(us, dx, g, 1.0, order)
+        fdm.grad(us, dx, g, 1.0, order)
+        fdm.divergence(vs, dx, g, 1.0, order)
+
+    bounds = np.linspace(0, n, threads + 1).astype(int)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        for _ in range(reps):
+            futs = []
+            for order in (2, 4):
+                g = order // 2
+                for i in range(threads):
+                    if bounds[i + 1] > bounds[i]:
+                        futs.append(ex.submit(slab_job, order, g + bounds[i], g + bounds[i + 1]))
+            for f in futs:
+                f.result()
+    dt = time.perf_counter() - t0
+    return 6 * n ** 3 * reps / dt, dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    n = 96
+    for _ in range(args.warmup):
+        cpu_sweep_sample(n, threads)
+    vals = []
+    t_all = 0.0
+    for _ in range(args.steps):
+        v, dt = cpu_sweep_sample(n, threads)
+        vals.append(v)
+        t_all += dt
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / max(args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "3D operator sweep, bounded CPU sample", "interior": [n, n, n],
+                   "ops_per_step": 6, "orders": [2, 4]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"the 6-operator step on a {n}^3 interior (order 2 and 4), NumPy float32 "
+                                   f"restatement of the reference kernels, X slabs over {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU ---
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    import pde_module_b200 as P
+    from pde_module_b200 import _lib
+
+    dx = 1.0 / N_INT
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1 + rank)
+    fields = {}
+    for order in (2, 4):
+        g = order // 2
+        s = N_INT + 2 * g
+        u = torch.randn((s, s, s, 1), device="cuda", generator=gen)
+        v = torch.randn((s, s, s, 3), device="cuda", generator=gen)
+        for f in (u, v):
+            bc = P.GridBoundary(f, dx, g)
+            bc.periodic("ALL" if world == 1 else ("Y", "Z"))
+            f.copy_(bc(f))
+        if world > 1:
+            exchange_x_halos(u, g, rank, world)
+            exchange_x_halos(v, g, rank, world)
+        mods = (P.Laplacian(1, dx, g, order=order), P.Grad(1, u.shape, dx, g, order=order),
+                P.Divergence(3, v.shape, dx, g, order=order))
+        fields[order] = (u, v, mods)
+
+    ops = []
+    for order in (2, 4):
+        u, v, (lap, grd, div) = fields[order]
+        ops.append((f"laplacian_o{order}", lambda u=u, lap=lap: lap(u, 1.0), ALG_BYTES["laplacian"]))
+        ops.append((f"grad_o{order}", lambda u=u, grd=grd: grd(u, 1.0), ALG_BYTES["grad"]))
+        ops.append((f"divergence_o{order}", lambda v=v, div=div: div(v, 1.0), ALG_BYTES["divergence"]))
+
+    def step():
+        for _, fn, _ in ops:
+            fn()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    if _lib.device_error() != 0:
+        raise RuntimeError("device error during warm-up")
+
+    stream = torch.cuda.current_stream()
+    K = args.steps
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in ops]
+          for _ in range(K)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    t0.record(stream)
+    for k in range(K):
+        for j, (_, fn, _) in enumerate(ops):
+            ev[k][j][0].record(stream)
+            fn()
+            ev[k][j][1].record(stream)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    per_op = {name: statistics.mean(ev[k][j][0].elapsed_time(ev[k][j][1]) for k in range(K))
+              for j, (name, _, _) in enumerate(ops)}
+    cells = N_INT ** 3
+    ms_step = ms / K
+    value = world * cells * len(ops) / (ms_step / 1000.0)
+
+    peak, peak_kind = peaks()
+    traffic = traffic_table()
+    kern = {}
+    for name, _, b in ops:
+        gbs = cells * b / (per_op[name] / 1000.0) / 1e9
+        kern[name] = {"ms": round(per_op[name], 4), "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    dom = max(per_op, key=per_op.get)
+    dom_b = dict((n, b) for n, _, b in ops)[dom]
+    ach = cells * dom_b / (per_op[dom] / 1000.0) / 1e9
+    tr = traffic.get(dom)
+    roofline = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": tr, "kernel": dom, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": cells * dom_b}
+
+    # end to end through the public API: pinned host fields in, all outputs back
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(fields, ops, world, args)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = os.cpu_count() or 1
+        v, dt = cpu_sweep_sample(96, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"the 6-operator step on a 96^3 interior, NumPy float32 restatement of the reference "
+                         f"kernels (oracle/fdm.py), X slabs over {threads} threads, {dt:.2f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic (standard normal, seeded)",
+            "config": {"workload": "3D operator sweep 512^3 (Laplacian, Grad, Divergence; order 2 and 4; "
+                                   "periodic ghosts)", "interior": [N_INT, N_INT, N_INT],
+                       "ops_per_step": len(ops), "fields": "scalar (512+2g)^3 and vec3 (512+2g)^3 per order",
+                       "l2": "inputs larger than L2 (>=543 MB each), no flush",
+                       "parallelism": f"dp{world}" if world > 1 else "single"},
+            "roofline": roofline, "kernels": kern, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": K * len(ops), "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def exchange_x_halos(f, g, rank, world):
+    """Periodic X ghost planes from the neighbouring ranks (once, before timing)."""
+    import torch
+    import torch.distributed as dist
+    left, right = (rank - 1) % world, (rank + 1) % world
+    n = f.shape[0]
+    send_lo = f[g:2 * g].contiguous()
+    send_hi = f[n - 2 * g:n - g].contiguous()
+    recv_lo = torch.empty_like(send_lo)
+    recv_hi = torch.empty_like(send_hi)
+    ops = [dist.P2POp(dist.isend, send_lo, left), dist.P2POp(dist.isend, send_hi, right),
+           dist.P2POp(dist.irecv, recv_hi, right), dist.P2POp(dist.irecv, recv_lo, left)]
+    for r in dist.batch_isend_irecv(ops):
+        r.wait()
+    f[0:g].copy_(recv_lo)
+    f[n - g:n].copy_(recv_hi)
+
+
+def run_e2e(fields, ops, world, args):
+    import torch
+    import torch.distributed as dist
+    host_in, dev_in, host_out = [], [], []
+    for order in (2, 4):
+        u, v, mods = fields[order]
+        for t in (u, v):
+            h = torch.empty(t.shape, dtype=t.dtype, pin_memory=True)
+            h.copy_(t)
+            host_in.append(h)
+            dev_in.append(t)
+        for m in mods:
+            if m.output_array is not None:
+                host_out.append((torch.empty(m.output_array.shape, dtype=torch.float32, pin_memory=True), m))
+    h2d = sum(h.numel() * 4 for h in host_in)
+    d2h = sum(h.numel() * 4 for h, _ in host_out)
+    K = max(1, min(args.steps, args.e2e_steps))
+    stream = torch.cuda.current_stream()
+
+    def e2e_step():
+        for h, d in zip(host_in, dev_in):
+            d.copy_(h, non_blocking=True)
+        for _, fn, _ in ops:
+            fn()
+        for h, m in host_out:
+            h.copy_(m.output_array, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(K):
+        e2e_step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    val = world * N_INT ** 3 * len(ops) / (ms / K / 1000.0)
+    return {"value": val, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": K,
+            "path": "pinned host fields -> H2D -> module calls (C ABI) -> D2H of every output"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,201 @@
+/*
+ * pde_b200.h -- C ABI of the B200 (sm_100a) finite-difference hot path.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream
+ * (passed as void*, i.e. a cudaStream_t; NULL = legacy default stream) and
+ * returns PDE_OK (0) or a negative PDE_ERR_* code.  Nothing aborts, nothing
+ * allocates device memory inside an operator call: scratch buffers and
+ * outputs are owned by the caller.
+ *
+ * Data layout (identical to PDE_Module's Warp `array3d(dtype=vec(N)/mat(N,D))`):
+ *   fp32, C-contiguous, shape (X, Y, Z, N) or (X, Y, Z, N, D); X, Y, Z include
+ *   the ghost layers; an axis of size 1 is not a spatial dimension (a 2D grid
+ *   is (X, Y, 1, ...)).  "Eligible" axes are those with size > 1, listed in
+ *   ascending order; D is their count.  Interior ("stencil") cells are the
+ *   indices [g, n-g) on every eligible axis (boundary nodes sit at g and n-g-1).
+ *
+ * Reference interfaces replaced (paths relative to the PDE_Module project):
+ *   pde_laplacian   FDM/functional/_laplacian.py:5-36 + FDM/kernel/laplacian.py:34-59
+ *   pde_grad        FDM/functional/_grad.py:5-36 + FDM/kernel/grad.py:37-102
+ *   pde_divergence  FDM/functional/_divergence.py:4-24 + FDM/kernel/divergence.py:32-106
+ *   pde_euler       time_step/forwardEuler.py:41-81
+ *   pde_bc_apply    FDM/boundary/functional_boundary.py:260-294 (copy + group launches)
+ *                   with the kernel of functional_boundary.py:312-402 and the value
+ *                   functions of FDM/boundary/boundary_functions.py:9-92
+ */
+#ifndef PDE_B200_H
+#define PDE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define PDE_OK                 0
+#define PDE_ERR_ARG          (-1)  /* null pointer / bad enum / bad count          */
+#define PDE_ERR_SHAPE        (-2)  /* shape inconsistent with the operator         */
+#define PDE_ERR_GHOST        (-3)  /* ghost width smaller than the stencil radius  */
+#define PDE_ERR_ALIGN        (-4)  /* pointer alignment requirement not met        */
+#define PDE_ERR_CUDA         (-5)  /* a CUDA runtime call failed                   */
+#define PDE_ERR_UNSUPPORTED  (-6)  /* valid request this build does not implement  */
+#define PDE_ERR_TIMEOUT      (-7)  /* a bounded device-side wait gave up           */
+#define PDE_ERR_TOO_LARGE    (-8)  /* size above a documented maximum              */
+
+/* Boundary-condition kinds: values of FDM/boundary/flags.py:8-16. */
+#define PDE_BC_DIRICHLET     1
+#define PDE_BC_VON_NEUMANN   2
+/* Boundary value functions: boundary_functions.py:9-47 (constant), :51-92 (ramp). */
+#define PDE_BC_FUNC_CONSTANT 0
+#define PDE_BC_FUNC_RAMP     1
+
+/* Face bits for standard boundary groups (functional_boundary.py:111-137). */
+#define PDE_FACE_XM  (1 << 0)  /* "-X" */
+#define PDE_FACE_XP  (1 << 1)  /* "+X" */
+#define PDE_FACE_YM  (1 << 2)  /* "-Y" */
+#define PDE_FACE_YP  (1 << 3)  /* "+Y" */
+#define PDE_FACE_ZM  (1 << 4)  /* "-Z" */
+#define PDE_FACE_ZP  (1 << 5)  /* "+Z" */
+
+/* Largest number of components a fused (boundary-in-the-stencil) kernel takes. */
+#define PDE_FUSED_MAX_COMP   4
+/* Largest number of boundary groups a compiled rule table holds. */
+#define PDE_MAX_GROUPS       16
+
+/* Uniform grid: array shape including ghosts, ghost width, stencil order, spacing.
+ * Stencil weights are formed on the host in double from dx and rounded to fp32,
+ * as the reference forms them (FDM/module/laplacian.py:33-35, grad.py:37-39,
+ * divergence.py:37-39):
+ *   Laplacian order 2: ( 1, -2,  1)/dx^2        order 4: (-1, 16, -30, 16, -1)/(12 dx^2)
+ *   first derivative order 2: (-1, 0, 1)/(2 dx) order 4: ( 1, -8,   0,  8, -1)/(12 dx)
+ * Order 4 has no reference counterpart (the reference rejects custom stencils). */
+typedef struct PdeGrid {
+  int64_t shape[3];     /* X, Y, Z including ghost layers                        */
+  int32_t ghost_cells;  /* g; must be >= order/2                                 */
+  int32_t order;        /* 2 or 4                                                */
+  double  dx;           /* grid spacing                                          */
+} PdeGrid;
+
+/* One boundary group (a FunctionBC of functional_boundary.py:25-55). */
+typedef struct PdeBCGroup {
+  const int32_t* node_ids;  /* device pointer: flat C-order node ids (X*Y*Z index) */
+  int32_t  count;           /* number of node ids                                  */
+  int32_t  type;            /* PDE_BC_DIRICHLET or PDE_BC_VON_NEUMANN              */
+  uint32_t comp_mask;       /* bit v set <=> component v is set (output_ids)       */
+  int32_t  func;            /* PDE_BC_FUNC_CONSTANT or PDE_BC_FUNC_RAMP            */
+  float    value;           /* constant (or ramp target)                           */
+  float    t_max;           /* ramp time scale (ramp only)                          */
+  int32_t  face_mask;       /* PDE_FACE_* bits when the group is a standard face
+                               group ("ALL" = every eligible face); 0 = custom ids */
+} PdeBCGroup;
+
+/* Boundary groups compiled for the fused kernels: for each node class (per
+ * axis: low node / other / high node, index kx*9+ky*3+kz) the group whose write
+ * wins at the node and at each adjacent ghost, per component; -1 = none.   */
+typedef struct PdeBCGroupParam {
+  int32_t  type;
+  uint32_t comp_mask;
+  int32_t  func;
+  float    value;
+  float    t_max;
+} PdeBCGroupParam;
+
+typedef struct PdeBCRules {
+  int32_t ncomp;
+  int32_t ngroups;
+  float   dx32;                               /* fp32 dx (ExplicitUniformGridStencil.py:27) */
+  int32_t has_ramp;                           /* any group uses a time-dependent value       */
+  PdeBCGroupParam group[PDE_MAX_GROUPS];
+  int8_t  node_group[27];                     /* last Dirichlet group containing the node    */
+  int8_t  ghost_group[27][3][PDE_FUSED_MAX_COMP]; /* last group setting ghost comp       */
+  int8_t  pad[1];
+} PdeBCRules;
+
+/* ---- library --------------------------------------------------------- */
+int         pde_version(void);
+const char* pde_strerror(int status);
+/* Reads and clears the device-side error word (bounded waits that gave up,
+ * bounds checks that failed).  0 = none.  Synchronises the given stream. */
+int         pde_device_error(void* stream);
+
+/* Kernel selection for pde_laplacian/pde_grad/pde_divergence: PDE_DISPATCH_AUTO
+ * picks the TMA streaming kernels where they apply, PDE_DISPATCH_GENERIC forces
+ * the general kernels (same arithmetic, used to cross-check the two bitwise).
+ * Process-wide; returns the previous mode. */
+#define PDE_DISPATCH_AUTO    0
+#define PDE_DISPATCH_GENERIC 1
+int         pde_set_dispatch(int mode);
+
+/* ---- operators (one launch each; out must not alias in) ------------- */
+
+/* out[c] = alpha * sum_{axis} sum_{tap} w[tap] * in[c + shift*e_axis], per component,
+ * for every interior cell c; ghost cells of out are not written.
+ * in/out: (X,Y,Z,ncomp).  Summation order: axes ascending, taps low to high,
+ * alpha last, every product and sum rounded separately (FDM/kernel/laplacian.py:34-46). */
+int pde_laplacian(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
+                  float alpha, void* stream);
+
+/* out[c][n][a] = alpha * sum_tap w[tap] * in[c + shift*e_axis(a)][n]
+ * in: (X,Y,Z,ncomp)  out: (X,Y,Z,ncomp,D)  (ncomp==1: the vec(D) output of Grad).
+ * FDM/kernel/grad.py:78-100. */
+int pde_grad(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
+             float alpha, void* stream);
+
+/* out[c][n] = alpha * sum_a sum_tap w[tap] * in[c + shift*e_axis(a)][n][a]
+ * in: (X,Y,Z,nrows,D) (nrows==1: vec(D) input)  out: (X,Y,Z,nrows).
+ * FDM/kernel/divergence.py:85-106.  One launch (the reference launches twice,
+ * FDM/module/divergence.py:98-110, with an identical result). */
+int pde_divergence(const float* in, float* out, const PdeGrid* grid, int32_t nrows,
+                   float alpha, void* stream);
+
+/* out[i] = y[i] + dt * k[i] for i < count (floats), time_step/forwardEuler.py:70-79. */
+int pde_euler(const float* y, const float* k, float dt, float* out, int64_t count,
+              void* stream);
+
+/* out = copy(in); then for each group in order: Dirichlet writes the node vector
+ * (input vector with the set components replaced by the value) and, for every
+ * eligible axis on which the node sits at index g or n-g-1, the ghost one step
+ * outside: ghost[v] = 2*val - in[adj][v]; Von Neumann writes only the ghost:
+ * ghost[v] = -sign(inc)*2*dx*val + in[adj][v].  t_device: device pointer to one
+ * float (time, ramp functions only; may be NULL when no group is a ramp).
+ * functional_boundary.py:260-294, 357-400. */
+int pde_bc_apply(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
+                 const PdeBCGroup* groups, int32_t ngroups, const float* t_device,
+                 void* stream);
+
+/* NEW (no reference counterpart: flags.py has no periodic kind).  In place:
+ * every ghost cell along the axes in axis_mask (bit a = axis a) takes the value
+ * of the interior cell congruent to it modulo the interior extent; axes are
+ * filled in ascending order over the full extent of the other axes, so edge and
+ * corner ghosts are filled too. */
+int pde_periodic_fill(float* u, const PdeGrid* grid, int32_t ncomp, int32_t axis_mask,
+                      void* stream);
+
+/* Host-only: compile standard face groups into the rule table the fused kernels
+ * read.  Fails with PDE_ERR_UNSUPPORTED when a group has face_mask == 0 (custom
+ * node lists) or ncomp > PDE_FUSED_MAX_COMP. */
+int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* grid,
+                   int32_t ncomp, PdeBCRules* rules_out);
+
+/* ---- fused explicit steps (boundary fill + Laplacian + forward Euler) ---- */
+
+/* nsteps of   u2 = BC(u);  u <- u2 + dt * (alpha * Laplacian(u2))   on a 2D or 3D
+ * grid, the composition of time_step/forwardEuler.py:41-61, FDM/module/laplacian.py
+ * and functional_boundary.py (examples/2D_Heat_Equation.py:57-65), bit-identical to
+ * running those three operators step by step.  Ghost cells of the result hold the
+ * boundary-filled values of the last step (the unfused chain leaves the same values
+ * when the Laplacian output's ghost cells are zero).
+ * u_in: initial field; u_out: result; work: scratch of the same size (used as the
+ * ping-pong buffer when nsteps > steps_per_pass).  u_out may equal u_in.
+ * steps_per_pass: temporal-blocking depth k (0 = choose).  2D (Z == 1) grids use
+ * shared-memory tiles with k steps per pass; 3D grids use k = 1.
+ * t0_device: device pointer to the time of the first step (ramp BCs), may be NULL. */
+int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                     int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
+                     int32_t nsteps, int32_t steps_per_pass, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDE_B200_H */

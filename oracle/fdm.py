@@ -1,0 +1,290 @@
+"""ORACLE — TEST INFRASTRUCTURE ONLY.
+
+CPU (NumPy) restatement of PDE_Module's finite-difference hot path, used by
+tests/, by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the
+checker.  Nothing in pde_module_b200 imports it.
+
+It follows the reference kernels operation by operation so that, in float32,
+every product and sum is rounded exactly where the reference's Warp kernel
+rounds it (no fused multiply-add):
+
+* Laplacian  — FDM/kernel/laplacian.py:34-59: ``acc = 0; for axis in
+  eligible axes: for tap: acc += w[tap] * u[c + shift*e_axis]; out = alpha*acc``
+  over the interior launch domain (functional/_laplacian.py:26-35);
+  weights FDM/module/laplacian.py:33-35, formed in float64, rounded to float32.
+* Grad       — FDM/kernel/grad.py:78-100 (weights module/grad.py:37-39).
+* Divergence — FDM/kernel/divergence.py:85-106 (weights module/divergence.py:37-39).
+* ForwardEuler — time_step/forwardEuler.py:70-79 (``cur + dt*k``, flat).
+* GridBoundary — groups functional_boundary.py:111-137; copy :260-263; per
+  group kernel :357-400 with the constant value function
+  boundary_functions.py:32-45 and the ramp :77-92.
+
+Order-4 weights and the periodic fill have no reference counterpart; they
+are restated from their definitions.  Pass ``dtype=np.float64`` for the
+float64 oracle (same operation order, double rounding).
+
+Parity pin: the reference package imports ``warp`` (warp-lang 1.12.1, not
+installed here), so its kernels are executed through the Warp-DSL emulator in
+oracle/warp_emu.py by tests/golden/make_golden.py; the fixtures it writes pin
+this restatement (tests/test_oracle_golden.py).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+DIRICHLET = 1
+VON_NEUMANN = 2
+
+
+# ---------------------------------------------------------------- weights ---
+def lap_weights(order: int, dx: float, dtype=np.float32) -> np.ndarray:
+    if order == 2:
+        w = [1.0 / dx ** 2, -2.0 / dx ** 2, 1.0 / dx ** 2]
+    elif order == 4:
+        d = 12.0 * dx * dx
+        w = [-1.0 / d, 16.0 / d, -30.0 / d, 16.0 / d, -1.0 / d]
+    else:
+        raise ValueError(order)
+    return np.array(w, dtype=np.float64).astype(dtype)
+
+
+def d1_weights(order: int, dx: float, dtype=np.float32) -> np.ndarray:
+    if order == 2:
+        w = [-1.0 / (2 * dx), 0.0, 1.0 / (2 * dx)]
+    elif order == 4:
+        d = 12.0 * dx
+        w = [1.0 / d, -8.0 / d, 0.0, 8.0 / d, -1.0 / d]
+    else:
+        raise ValueError(order)
+    return np.array(w, dtype=np.float64).astype(dtype)
+
+
+# ----------------------------------------------------------------- shapes ---
+def eligible_dims(grid_shape) -> tuple:
+    return tuple(i for i, s in enumerate(grid_shape[:3]) if s > 1)
+
+
+def _interior_slices(grid_shape, g, shift=(0, 0, 0)):
+    """Slices of the interior launch domain moved by ``shift`` cells."""
+    sl = []
+    for a in range(3):
+        n = grid_shape[a]
+        if n > 1:
+            sl.append(slice(g + shift[a], n - g + shift[a]))
+        else:
+            sl.append(slice(0, n))
+    return tuple(sl)
+
+
+# -------------------------------------------------------------- operators ---
+def laplacian(u: np.ndarray, dx: float, ghost: int, alpha: float, order: int = 2, dtype=np.float32,
+              out: np.ndarray | None = None) -> np.ndarray:
+    """u: (X, Y, Z, N).  Returns out with the interior written (ghosts 0)."""
+    u = np.asarray(u, dtype=dtype)
+    w = lap_weights(order, dx, dtype)
+    R = (len(w) - 1) // 2
+    gs = u.shape[:3]
+    if out is None:
+        out = np.zeros_like(u)
+    core = _interior_slices(gs, ghost)
+    acc = np.zeros(u[core].shape, dtype=dtype)
+    for a in eligible_dims(gs):
+        for t in range(len(w)):
+            sh = [0, 0, 0]
+            sh[a] = t - R
+            acc = acc + w[t] * u[_interior_slices(gs, ghost, sh)]
+    out[core] = dtype(alpha) * acc
+    return out
+
+
+def grad(u: np.ndarray, dx: float, ghost: int, alpha: float, order: int = 2, dtype=np.float32,
+         force_matrix: bool = False) -> np.ndarray:
+    """u: (X, Y, Z, N) -> (X, Y, Z, N, D), or (X, Y, Z, D) when N == 1 and not force_matrix."""
+    u = np.asarray(u, dtype=dtype)
+    w = d1_weights(order, dx, dtype)
+    R = (len(w) - 1) // 2
+    gs = u.shape[:3]
+    dims = eligible_dims(gs)
+    N = u.shape[3]
+    out = np.zeros(gs + (N, len(dims)), dtype=dtype)
+    core = _interior_slices(gs, ghost)
+    for col, a in enumerate(dims):
+        acc = np.zeros(u[core].shape, dtype=dtype)
+        for t in range(len(w)):
+            sh = [0, 0, 0]
+            sh[a] = t - R
+            acc = acc + w[t] * u[_interior_slices(gs, ghost, sh)]
+        out[core + (slice(None), col)] = dtype(alpha) * acc
+    if N == 1 and not force_matrix:
+        out = out[:, :, :, 0, :].copy()
+    return out
+
+
+def divergence(u: np.ndarray, dx: float, ghost: int, alpha: float, order: int = 2,
+               dtype=np.float32) -> np.ndarray:
+    """u: (X, Y, Z, D) vector -> (X, Y, Z, 1); (X, Y, Z, N, D) matrix -> (X, Y, Z, N)."""
+    u = np.asarray(u, dtype=dtype)
+    if u.ndim == 4:
+        u = u[:, :, :, None, :]
+    w = d1_weights(order, dx, dtype)
+    R = (len(w) - 1) // 2
+    gs = u.shape[:3]
+    dims = eligible_dims(gs)
+    N = u.shape[3]
+    assert u.shape[4] == len(dims)
+    out = np.zeros(gs + (N,), dtype=dtype)
+    core = _interior_slices(gs, ghost)
+    acc = np.zeros(u[core][..., 0].shape, dtype=dtype)
+    for col, a in enumerate(dims):
+        for t in range(len(w)):
+            sh = [0, 0, 0]
+            sh[a] = t - R
+            acc = acc + w[t] * u[_interior_slices(gs, ghost, sh)][..., col]
+    out[core] = dtype(alpha) * acc
+    return out
+
+
+def forward_euler(y: np.ndarray, k: np.ndarray, dt: float, dtype=np.float32) -> np.ndarray:
+    y = np.asarray(y, dtype=dtype)
+    k = np.asarray(k, dtype=dtype)
+    return y + dtype(dt) * k
+
+
+# --------------------------------------------------------------- boundary ---
+def exterior_groups(grid_shape, ghost: int) -> dict:
+    """Node-id groups of functional_boundary.py:111-137 (C-order flat ids)."""
+    gs = tuple(grid_shape[:3])
+    ids = np.arange(int(np.prod(gs)), dtype=np.int32).reshape(gs)
+    groups, faces = {}, []
+    for i, ax in enumerate("XYZ"):
+        if gs[i] <= 1:
+            continue
+        for prefix in "-+":
+            sl = [slice(None)] * 3
+            sl[i] = ghost if prefix == "-" else -(ghost + 1)
+            for x in range(3):
+                if gs[x] > 1 and x != i:
+                    sl[x] = slice(ghost, -ghost) if ghost > 0 else slice(None)
+            groups[prefix + ax] = ids[tuple(sl)].ravel()
+            faces.append(groups[prefix + ax])
+    groups["ALL"] = np.unique(np.concatenate(faces)).astype(np.int32)
+    return groups
+
+
+def bc_value(func: str, value: float, t: float = 0.0, t_max: float = 1.0, dtype=np.float32):
+    v = dtype(value)
+    if func == "ramp":
+        ramp = np.minimum(dtype(t) / dtype(t_max), dtype(1.0))
+        return dtype(ramp * v)
+    return v
+
+
+def bc_apply(u: np.ndarray, groups: list, dx: float, ghost: int, t: float = 0.0,
+             dtype=np.float32) -> np.ndarray:
+    """Copy, then each group in order.
+
+    groups: list of dicts {ids, type (1/2), comps (tuple), func ('constant'|'ramp'), value, t_max}.
+    Reads only the pre-boundary field ``u``.
+    """
+    u = np.asarray(u, dtype=dtype)
+    out = u.copy()
+    gs = u.shape[:3]
+    dims = eligible_dims(gs)
+    N = u.shape[3]
+    dx32 = dtype(dx)
+    flat_u = u.reshape(-1, N)
+    flat_o = out.reshape(-1, N)
+    strides = (gs[1] * gs[2], gs[2], 1)
+    for G in groups:
+        ids = np.asarray(G["ids"], dtype=np.int64)
+        if ids.size == 0:
+            continue
+        ijk = np.stack([ids // (gs[1] * gs[2]), (ids // gs[2]) % gs[1], ids % gs[2]], axis=1)
+        v = bc_value(G.get("func", "constant"), G["value"], t, G.get("t_max", 1.0), dtype)
+        comps = tuple(G["comps"])
+        if G["type"] == DIRICHLET:
+            node_vals = flat_u[ids].copy()
+            for c in comps:
+                node_vals[:, c] = v
+            flat_o[ids] = node_vals
+        for a in dims:
+            inc = np.zeros(len(ids), dtype=np.int64)
+            inc[ijk[:, a] == ghost] = 1
+            inc[(ijk[:, a] == gs[a] - 1 - ghost) & (inc == 0)] = -1
+            sel = inc != 0
+            if not sel.any():
+                continue
+            ghost_ids = ids[sel] - inc[sel] * strides[a]
+            adj_ids = ids[sel] + inc[sel] * strides[a]
+            for c in comps:
+                cur = flat_u[adj_ids, c]
+                if G["type"] == DIRICHLET:
+                    nv = dtype(2.0) * v - cur
+                else:
+                    s = (-np.sign(inc[sel]).astype(dtype)) * dtype(2.0)
+                    nv = s * dx32 * v + cur
+                flat_o[ghost_ids, c] = nv
+    return out
+
+
+def periodic_fill(u: np.ndarray, ghost: int, axes) -> np.ndarray:
+    """New (no reference counterpart): wrap every ghost layer along ``axes``,
+    axes processed in ascending order over the full extent of the others."""
+    out = np.array(u, copy=True)
+    gs = out.shape[:3]
+    for a in sorted(axes):
+        n = gs[a]
+        M = n - 2 * ghost
+        src = [ghost + ((i - ghost) % M) for i in range(n)]
+        idx = [slice(None)] * 3
+        for i in list(range(ghost)) + list(range(n - ghost, n)):
+            idx_d = list(idx)
+            idx_s = list(idx)
+            idx_d[a] = i
+            idx_s[a] = src[i]
+            out[tuple(idx_d)] = out[tuple(idx_s)]
+    return out
+
+
+# ------------------------------------------------------------- rollouts ---
+def heat_step(u: np.ndarray, groups: list, dx: float, ghost: int, alpha: float, dt: float, order: int = 2,
+              dtype=np.float32) -> np.ndarray:
+    """One step of examples/2D_Heat_Equation.py:59-62 with a zero-ghost Laplacian output."""
+    u2 = bc_apply(u, groups, dx, ghost, dtype=dtype)
+    lap = laplacian(u2, dx, ghost, alpha, order, dtype)
+    return forward_euler(u2, lap, dt, dtype)
+
+
+def heat_rollout(u: np.ndarray, groups: list, dx: float, ghost: int, alpha: float, dt: float, nsteps: int,
+                 order: int = 2, dtype=np.float32) -> np.ndarray:
+    u = np.asarray(u, dtype=dtype)
+    for _ in range(nsteps):
+        u = heat_step(u, groups, dx, ghost, alpha, dt, order, dtype)
+    return u
+
+
+def standard_groups(grid_shape, ghost, spec) -> list:
+    """spec: list of (group_name, type, value, comps) -> group dicts with ids."""
+    G = exterior_groups(grid_shape, ghost)
+    return [dict(ids=G[name], type=typ, value=val, comps=tuple(comps), func="constant")
+            for name, typ, val, comps in spec]
+
+
+# ------------------------------------------------------ per-cell samples ---
+def stencil_at(u: np.ndarray, cells: np.ndarray, w: np.ndarray, axes_comps, alpha: float,
+               dtype=np.float32) -> np.ndarray:
+    """Reference-order stencil sum at selected cells.
+
+    u: (X, Y, Z, C) array (C = flattened trailing components); cells: (M, 3)
+    int array; axes_comps: list of (axis, component) pairs visited in order,
+    each contributing its taps low to high into one accumulator per cell.
+    Used to check full-size (e.g. 512^3) outputs at sampled cells.
+    """
+    R = (len(w) - 1) // 2
+    acc = np.zeros(len(cells), dtype=dtype)
+    for a, comp in axes_comps:
+        for t in range(len(w)):
+            idx = cells.copy()
+            idx[:, a] += t - R
+            acc = acc + w[t] * u[idx[:, 0], idx[:, 1], idx[:, 2], comp]
+    return dtype(alpha) * acc

@@ -1,0 +1,13 @@
+"""pde_module_b200: the finite-difference hot path of PDE_Module on B200 (sm_100a).
+
+Drop-in module API (Laplacian, Grad, Divergence, GridBoundary, ForwardEuler and
+their functional forms) over torch CUDA float32 tensors, backed by the C ABI
+of include/pde_b200.h in ``_native/libpde_b200.so``.
+"""
+from . import _lib
+from .FDM import Laplacian, Grad, Divergence, GridBoundary
+from .time_step import ForwardEuler, HeatRollout
+from .mesh import UniformGridMesh, create_structured_field, create_structured_warp_field
+
+__all__ = ["Laplacian", "Grad", "Divergence", "GridBoundary", "ForwardEuler", "HeatRollout",
+           "UniformGridMesh", "create_structured_field", "create_structured_warp_field"]

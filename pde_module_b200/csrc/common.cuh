@@ -1,0 +1,109 @@
+// Shared helpers for the sm_100a kernels of the finite-difference hot path.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/pde_b200.h"
+
+namespace pde {
+
+// Geometry of one (X, Y, Z, N...) array, derived from PdeGrid.
+struct Geo {
+  int64_t n[3];        // array extents including ghosts
+  int64_t lo[3];       // first interior index per axis (g on eligible axes, else 0)
+  int64_t ext[3];      // interior extent per axis (n - 2g on eligible axes, else n)
+  int64_t cstride[3];  // cell strides: Y*Z, Z, 1
+  int ndims;           // number of eligible axes
+  int dims[3];         // eligible axes, ascending
+  int g;
+  int order;
+};
+
+// Stencil weights rounded to fp32, largest stencil is 5 taps.
+struct Weights {
+  float w[5];
+  int taps;  // 3 or 5
+  int radius;
+};
+
+inline bool make_geo(const PdeGrid* grid, Geo* geo) {
+  if (!grid) return false;
+  if (grid->order != 2 && grid->order != 4) return false;
+  if (grid->ghost_cells < 0) return false;
+  geo->g = grid->ghost_cells;
+  geo->order = grid->order;
+  geo->ndims = 0;
+  for (int a = 0; a < 3; ++a) {
+    if (grid->shape[a] < 1) return false;
+    geo->n[a] = grid->shape[a];
+  }
+  geo->cstride[2] = 1;
+  geo->cstride[1] = geo->n[2];
+  geo->cstride[0] = geo->n[1] * geo->n[2];
+  for (int a = 0; a < 3; ++a) {
+    if (geo->n[a] > 1) {
+      geo->dims[geo->ndims++] = a;
+      geo->lo[a] = geo->g;
+      geo->ext[a] = geo->n[a] - 2 * (int64_t)geo->g;
+      if (geo->ext[a] < 1) return false;
+    } else {
+      geo->lo[a] = 0;
+      geo->ext[a] = geo->n[a];
+    }
+  }
+  for (int k = geo->ndims; k < 3; ++k) geo->dims[k] = -1;
+  return geo->ndims >= 1;
+}
+
+// Laplacian weights: order 2 (1,-2,1)/dx^2 (FDM/module/laplacian.py:33-35);
+// order 4 (-1,16,-30,16,-1)/(12 dx^2).  Formed in double, rounded to fp32.
+inline Weights lap_weights(int order, double dx) {
+  Weights W{};
+  if (order == 2) {
+    double d2 = dx * dx;
+    W.taps = 3; W.radius = 1;
+    W.w[0] = (float)(1.0 / d2); W.w[1] = (float)(-2.0 / d2); W.w[2] = (float)(1.0 / d2);
+  } else {
+    double d = 12.0 * dx * dx;
+    W.taps = 5; W.radius = 2;
+    W.w[0] = (float)(-1.0 / d); W.w[1] = (float)(16.0 / d); W.w[2] = (float)(-30.0 / d);
+    W.w[3] = (float)(16.0 / d); W.w[4] = (float)(-1.0 / d);
+  }
+  return W;
+}
+
+// First-derivative weights: order 2 (-1,0,1)/(2dx) (FDM/module/grad.py:37-39,
+// divergence.py:37-39); order 4 (1,-8,0,8,-1)/(12 dx).
+inline Weights d1_weights(int order, double dx) {
+  Weights W{};
+  if (order == 2) {
+    W.taps = 3; W.radius = 1;
+    W.w[0] = (float)(-1.0 / (2 * dx)); W.w[1] = 0.0f; W.w[2] = (float)(1.0 / (2 * dx));
+  } else {
+    double d = 12.0 * dx;
+    W.taps = 5; W.radius = 2;
+    W.w[0] = (float)(1.0 / d); W.w[1] = (float)(-8.0 / d); W.w[2] = 0.0f;
+    W.w[3] = (float)(8.0 / d); W.w[4] = (float)(-1.0 / d);
+  }
+  return W;
+}
+
+// Correctly rounded fp32 operations that the compiler may not contract into FMA:
+// every product and every sum of the reference is rounded on its own.
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+
+inline int grid_blocks(int64_t work, int threads, int64_t cap = 148LL * 64) {
+  int64_t b = (work + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+
+}  // namespace pde
+
+#define PDE_CUDA_CHECK(expr)                    \
+  do {                                          \
+    cudaError_t _e = (expr);                    \
+    if (_e != cudaSuccess) return PDE_ERR_CUDA; \
+  } while (0)

@@ -1,0 +1,256 @@
+// Fused explicit steps: ghost/boundary fill + Laplacian + forward Euler in one
+// pass, with the boundary groups compiled into a PdeBCRules table.
+//
+// The per-cell boundary semantics are those of functional_boundary.py:357-400
+// applied group by group: a boundary node takes the vector of the last
+// Dirichlet group that contains it (input vector with that group's components
+// replaced); the ghost one step outside a node along an axis takes, per
+// component, the formula of the last group containing the node that sets the
+// component, evaluated on the pre-boundary field at the interior neighbour
+// (adj = node + inc).  All other cells keep the input value.
+#pragma once
+#include "common.cuh"
+#include "generic.cuh"
+
+namespace pde {
+
+__device__ __forceinline__ int node_class_axis(int64_t i, int64_t n, int g, bool elig) {
+  if (!elig) return 1;
+  if (i == g) return 0;
+  if (i == n - 1 - g) return 2;
+  return 1;
+}
+
+// Value written into a ghost component by group `gi` from the pre-boundary
+// neighbour value `a` (inc = +1 for a low-side node, -1 for a high-side node).
+__device__ __forceinline__ float ghost_value(const PdeBCRules& Rl, int gi, int inc, float a) {
+  const PdeBCGroupParam& G = Rl.group[gi];
+  const float v = G.value;  // constant groups only on fused paths
+  if (G.type == PDE_BC_DIRICHLET) return sub(mul(2.0f, v), a);
+  return add(mul(mul((float)(-2 * inc), Rl.dx32), v), a);
+}
+
+// Boundary-filled value u2 at cell (c0,c1,c2), component v, of the field
+// `u` (pre-boundary), read through accessor U(i,j,k,v).
+template <class Acc>
+__device__ __forceinline__ float bc_eval(const Geo& G, const PdeBCRules& Rl, const Acc& U, int64_t c0, int64_t c1,
+                                         int64_t c2, int v) {
+  const int64_t c[3] = {c0, c1, c2};
+  int ghost_axis = -1, nghost = 0;
+  bool deep = false;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (G.n[a] == 1) continue;
+    if (c[a] < G.g || c[a] > G.n[a] - 1 - G.g) {
+      if (c[a] == G.g - 1 || c[a] == G.n[a] - G.g) { ghost_axis = a; ++nghost; }
+      else deep = true;
+    }
+  }
+  if (deep || nghost > 1) return U(c0, c1, c2, v);
+  if (nghost == 1) {
+    const int a = ghost_axis;
+    const int inc = (c[a] == G.g - 1) ? 1 : -1;
+    int64_t p[3] = {c0, c1, c2};
+    p[a] += inc;  // partner node
+    const int K = node_class_axis(p[0], G.n[0], G.g, G.n[0] > 1) * 9 +
+                  node_class_axis(p[1], G.n[1], G.g, G.n[1] > 1) * 3 +
+                  node_class_axis(p[2], G.n[2], G.g, G.n[2] > 1);
+    const int gi = Rl.ghost_group[K][a][v];
+    if (gi < 0) return U(c0, c1, c2, v);
+    p[a] += inc;  // adj = node + inc
+    return ghost_value(Rl, gi, inc, U(p[0], p[1], p[2], v));
+  }
+  const int K = node_class_axis(c0, G.n[0], G.g, G.n[0] > 1) * 9 + node_class_axis(c1, G.n[1], G.g, G.n[1] > 1) * 3 +
+                node_class_axis(c2, G.n[2], G.g, G.n[2] > 1);
+  if (K != 13) {
+    const int gi = Rl.node_group[K];
+    if (gi >= 0 && ((Rl.group[gi].comp_mask >> v) & 1u)) return Rl.group[gi].value;
+  }
+  return U(c0, c1, c2, v);
+}
+
+struct GlobalAcc {
+  const float* u;
+  int64_t s0, s1;  // cell strides
+  int N;
+  __device__ __forceinline__ float operator()(int64_t i, int64_t j, int64_t k, int v) const {
+    return __ldg(u + (i * s0 + j * s1 + k) * N + v);
+  }
+};
+
+// One fused step over the whole array (any number of eligible axes), thread
+// per (cell, component): stencil cells get u2 + dt*(alpha*L(u2)); every other
+// cell gets u2 (its boundary-filled value).
+template <int R>
+__global__ void __launch_bounds__(256) heat_step_kernel(const float* __restrict__ in, float* __restrict__ out, Geo G,
+                                                        int N, Weights W, float alpha, float dt, const PdeBCRules Rl,
+                                                        int64_t total) {
+  GlobalAcc U{in, G.cstride[0], G.cstride[1], N};
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t cell = t / N;
+    const int v = (int)(t - cell * N);
+    const int64_t c2 = cell % G.n[2];
+    const int64_t r = cell / G.n[2];
+    const int64_t c1 = r % G.n[1];
+    const int64_t c0 = r / G.n[1];
+    const float u2 = bc_eval(G, Rl, U, c0, c1, c2, v);
+    bool st = true;
+    const int64_t c[3] = {c0, c1, c2};
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+      if (G.n[a] > 1 && (c[a] < G.g || c[a] >= G.n[a] - G.g)) st = false;
+    float res = u2;
+    if (st) {
+      float acc = 0.0f;
+      for (int d = 0; d < G.ndims; ++d) {
+        const int a = G.dims[d];
+#pragma unroll
+        for (int tp = 0; tp < 2 * R + 1; ++tp) {
+          int64_t q[3] = {c0, c1, c2};
+          q[a] += tp - R;
+          acc = add(acc, mul(W.w[tp], bc_eval(G, Rl, U, q[0], q[1], q[2], v)));
+        }
+      }
+      res = add(u2, mul(dt, mul(alpha, acc)));
+    }
+    out[cell * N + v] = res;
+  }
+}
+
+// ---- 2D temporal blocking -------------------------------------------------
+struct H2Params {
+  int X, Y, g, N;
+  int k;           // steps in this pass
+  int TBX, TBY;    // output tile (array coordinates, ghosts included)
+  int tiles_y;
+  int RXM, RYM;    // smem region capacity (cells)
+  float w[5];
+  float alpha, dt;
+};
+
+// Boundary fill of the smem region (array rectangle [rx0,rx0+RX) x [ry0,ry0+RY)),
+// in place: ghosts first (they read pre-boundary interior values), then nodes.
+template <int N>
+__device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, const PdeBCRules& Rl, int rx0, int RX,
+                                               int ry0, int RY) {
+  const int g = P.g, X = P.X, Y = P.Y;
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  // ghost strips: x = g-1 (low), x = X-g (high), partner rows y in [g, Y-g)
+  const int ylo = max(g, ry0), yhi = min(Y - g, ry0 + RY);
+  const int xlo = max(g, rx0), xhi = min(X - g, rx0 + RX);
+  const int ny = max(0, yhi - ylo), nx = max(0, xhi - xlo);
+  const int total = 2 * ny + 2 * nx;
+  for (int e = tid; e < total; e += nthr) {
+    int gx, gy, ax, inc;
+    if (e < 2 * ny) {
+      const int side = e / ny;
+      gy = ylo + (e - side * ny);
+      gx = side == 0 ? g - 1 : X - g;
+      inc = side == 0 ? 1 : -1;
+      ax = 0;
+    } else {
+      const int e2 = e - 2 * ny;
+      const int side = e2 / nx;
+      gx = xlo + (e2 - side * nx);
+      gy = side == 0 ? g - 1 : Y - g;
+      inc = side == 0 ? 1 : -1;
+      ax = 1;
+    }
+    const int px = gx + (ax == 0 ? inc : 0), py = gy + (ax == 1 ? inc : 0);
+    const int qx = px + (ax == 0 ? inc : 0), qy = py + (ax == 1 ? inc : 0);
+    if (gx < rx0 || gx >= rx0 + RX || gy < ry0 || gy >= ry0 + RY) continue;
+    if (qx < rx0 || qx >= rx0 + RX || qy < ry0 || qy >= ry0 + RY) continue;
+    const int K = node_class_axis(px, X, g, true) * 9 + node_class_axis(py, Y, g, true) * 3 + 1;
+#pragma unroll
+    for (int v = 0; v < N; ++v) {
+      const int gi = Rl.ghost_group[K][ax][v];
+      if (gi < 0) continue;
+      const float a = A[((qx - rx0) * RY + (qy - ry0)) * N + v];
+      A[((gx - rx0) * RY + (gy - ry0)) * N + v] = ghost_value(Rl, gi, inc, a);
+    }
+  }
+  __syncthreads();
+  // node strips: x in {g, X-g-1} (y in [g,Y-g)), y in {g, Y-g-1} (x in [g,X-g))
+  for (int e = tid; e < total; e += nthr) {
+    int x, y;
+    if (e < 2 * ny) {
+      const int side = e / ny;
+      y = ylo + (e - side * ny);
+      x = side == 0 ? g : X - g - 1;
+    } else {
+      const int e2 = e - 2 * ny;
+      const int side = e2 / nx;
+      x = xlo + (e2 - side * nx);
+      y = side == 0 ? g : Y - g - 1;
+    }
+    if (x < rx0 || x >= rx0 + RX || y < ry0 || y >= ry0 + RY) continue;
+    const int K = node_class_axis(x, X, g, true) * 9 + node_class_axis(y, Y, g, true) * 3 + 1;
+    const int gi = Rl.node_group[K];
+    if (gi < 0) continue;
+    const uint32_t m = Rl.group[gi].comp_mask;
+    const float val = Rl.group[gi].value;
+#pragma unroll
+    for (int v = 0; v < N; ++v)
+      if ((m >> v) & 1u) A[((x - rx0) * RY + (y - ry0)) * N + v] = val;
+  }
+  __syncthreads();
+}
+
+// k fused steps on a 2D grid (X, Y, 1, N) per pass.  Tiles cover the whole
+// array (ghosts included); the smem region is the tile grown by k*R cells on
+// each side (clipped to the array).  After k sub-steps the tile itself is
+// exact: garbage enters only from the region's cut edges, R cells per step.
+template <int R, int N>
+__global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                        const H2Params P, const PdeBCRules Rl) {
+  extern __shared__ __align__(16) float sm[];
+  const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
+  const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
+  const int H = P.k * R;
+  const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, P.X);
+  const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
+  const int RX = rx1 - rx0, RY = ry1 - ry0;
+  float* A = sm;
+  float* B = sm + P.RXM * P.RYM * N;
+  const int nrow = RY * N, ncell = RX * nrow;
+  for (int idx = threadIdx.x; idx < ncell; idx += blockDim.x) {
+    const int lx = idx / nrow, rem = idx - lx * nrow;
+    A[idx] = __ldg(in + ((size_t)(rx0 + lx) * P.Y + ry0) * N + rem);
+  }
+  __syncthreads();
+  const int g = P.g;
+  for (int s = 0; s < P.k; ++s) {
+    bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY);
+    for (int idx = threadIdx.x; idx < ncell; idx += blockDim.x) {
+      const int lx = idx / nrow, rem = idx - lx * nrow;
+      const int ly = rem / N;
+      const int x = rx0 + lx, y = ry0 + ly;
+      const float u2 = A[idx];
+      float res = u2;
+      if (x >= g && x < P.X - g && y >= g && y < P.Y - g && lx >= R && lx < RX - R && ly >= R && ly < RY - R) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * nrow]));
+#pragma unroll
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * N]));
+        res = add(u2, mul(P.dt, mul(P.alpha, acc)));
+      }
+      B[idx] = res;
+    }
+    __syncthreads();
+    float* tmp = A;
+    A = B;
+    B = tmp;
+  }
+  // The ghost cells of the result hold the last step's boundary-filled values,
+  // which B (the pre-step buffer) already has; A holds u2 copied through.
+  const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
+  const int onrow = (oy1 - by0) * N, on = (ox1 - bx0) * onrow;
+  for (int idx = threadIdx.x; idx < on; idx += blockDim.x) {
+    const int lx = idx / onrow, rem = idx - lx * onrow;
+    const int x = bx0 + lx;
+    out[((size_t)x * P.Y + by0) * N + rem] = A[((x - rx0) * RY + (by0 - ry0)) * N + rem];
+  }
+}
+
+}  // namespace pde

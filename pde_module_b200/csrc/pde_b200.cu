@@ -1,0 +1,387 @@
+// C-ABI entry points of the finite-difference hot path (include/pde_b200.h).
+// One translation unit: every kernel header is included here so the library
+// has a single device-side error word.
+#include <cuda_runtime.h>
+#include <string.h>
+
+#include "common.cuh"
+#include "generic.cuh"
+#include "stream3d.cuh"
+#include "fused.cuh"
+
+using namespace pde;
+
+namespace {
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+  }
+  return n;
+}
+
+int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ERR_CUDA; }
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// ---- 3D streaming dispatch -------------------------------------------------
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
+int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt, float alpha, cudaStream_t st) {
+  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>;
+  auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF>;
+  static int occ = -1;
+  if (occ < 0) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM) != cudaSuccess)
+      return PDE_ERR_CUDA;
+    int o = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, C::THREADS, C::SMEM) != cudaSuccess || o < 1)
+      return PDE_ERR_CUDA;
+    occ = o;
+  }
+  const int64_t total = G.n[0] * G.n[1] * G.n[2] * CIN;
+  S3Params P;
+  P.X = (int)G.n[0]; P.Y = (int)G.n[1]; P.Z = (int)G.n[2]; P.g = G.g;
+  P.ny_tiles = (int)((G.ext[1] + TY - 1) / TY);
+  P.nz_tiles = (int)((G.ext[2] + TZ - 1) / TZ);
+  P.pp = (int)((G.n[1] * G.n[2] * CIN) & 3);
+  P.pr = (int)((G.n[2] * CIN) & 3);
+  for (int t = 0; t < 5; ++t) P.w[t] = Wt.w[t];
+  P.alpha = alpha;
+  P.out = out;
+  const int tiles = P.ny_tiles * P.nz_tiles;
+  const int resident = occ * sm_count();
+  int nchunks = resident / tiles;
+  if (nchunks < 1) nchunks = 1;
+  const int nx = (int)G.ext[0];
+  if (nchunks > nx) nchunks = nx;
+  P.chunk = (nx + nchunks - 1) / nchunks;
+  nchunks = (nx + P.chunk - 1) / P.chunk;
+  CUtensorMap m;
+  if (!encode_1d(&m, in, (uint64_t)total, (uint32_t)C::W)) return PDE_ERR_CUDA;
+  kern<<<tiles * nchunks, dim3(C::LANES, C::TYG), C::SMEM, st>>>(m, P);
+  return launch_status();
+}
+
+// The flat 1D TMA view addresses floats with int32 coordinates, including rows
+// up to one tile past the last interior row.
+int g_dispatch = PDE_DISPATCH_AUTO;
+
+bool stream3d_ok(const float* in, const Geo& G, int cin) {
+  if (g_dispatch == PDE_DISPATCH_GENERIC) return false;
+  if (G.ndims != 3) return false;
+  if (!aligned16(in)) return false;
+  const int64_t total = G.n[0] * G.n[1] * G.n[2] * cin;
+  const int64_t slack = 64LL * G.n[2] * cin + 1024;
+  return total + slack < (1LL << 31) && G.g >= G.order / 2;
+}
+
+int check_common(const void* in, const void* out, const PdeGrid* grid, int ncomp, Geo* G) {
+  if (!in || !out || !grid) return PDE_ERR_ARG;
+  if (ncomp < 1) return PDE_ERR_ARG;
+  if (!make_geo(grid, G)) return PDE_ERR_SHAPE;
+  if (G->g < G->order / 2) return PDE_ERR_GHOST;
+  if (in == out) return PDE_ERR_ARG;
+  return PDE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pde_version(void) { return 100; }
+
+int pde_set_dispatch(int mode) {
+  const int prev = g_dispatch;
+  if (mode == PDE_DISPATCH_AUTO || mode == PDE_DISPATCH_GENERIC) g_dispatch = mode;
+  return prev;
+}
+
+const char* pde_strerror(int s) {
+  switch (s) {
+    case PDE_OK: return "ok";
+    case PDE_ERR_ARG: return "invalid argument";
+    case PDE_ERR_SHAPE: return "shape inconsistent with the operator";
+    case PDE_ERR_GHOST: return "ghost width smaller than the stencil radius";
+    case PDE_ERR_ALIGN: return "pointer alignment requirement not met";
+    case PDE_ERR_CUDA: return "CUDA runtime call failed";
+    case PDE_ERR_UNSUPPORTED: return "not supported by this build";
+    case PDE_ERR_TIMEOUT: return "a bounded device wait gave up";
+    case PDE_ERR_TOO_LARGE: return "size above the documented maximum";
+    default: return "unknown status";
+  }
+}
+
+int pde_device_error(void* stream) {
+  if (cudaStreamSynchronize(as_stream(stream)) != cudaSuccess) return PDE_ERR_CUDA;
+  int v = 0, z = 0;
+  if (cudaMemcpyFromSymbol(&v, g_err, sizeof(int)) != cudaSuccess) return PDE_ERR_CUDA;
+  if (cudaMemcpyToSymbol(g_err, &z, sizeof(int)) != cudaSuccess) return PDE_ERR_CUDA;
+  return v;
+}
+
+int pde_laplacian(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, void* stream) {
+  Geo G;
+  int rc = check_common(in, out, grid, ncomp, &G);
+  if (rc) return rc;
+  const Weights W = lap_weights(G.order, grid->dx);
+  cudaStream_t st = as_stream(stream);
+  if ((ncomp == 1 || ncomp == 3) && stream3d_ok(in, G, ncomp)) {
+    if (G.order == 2) {
+      if (ncomp == 1) return launch_stream3d<1, OP_LAP, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
+      return launch_stream3d<1, OP_LAP, 3, 32, 16, 4, 3>(in, out, G, W, alpha, st);
+    } else {
+      if (ncomp == 1) return launch_stream3d<2, OP_LAP, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
+      return launch_stream3d<2, OP_LAP, 3, 32, 16, 4, 3>(in, out, G, W, alpha, st);
+    }
+  }
+  const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp;
+  const int blocks = grid_blocks(total, 256);
+  if (G.order == 2) lap_generic_kernel<1><<<blocks, 256, 0, st>>>(in, out, G, ncomp, W, alpha, total);
+  else lap_generic_kernel<2><<<blocks, 256, 0, st>>>(in, out, G, ncomp, W, alpha, total);
+  return launch_status();
+}
+
+int pde_grad(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, void* stream) {
+  Geo G;
+  int rc = check_common(in, out, grid, ncomp, &G);
+  if (rc) return rc;
+  const Weights W = d1_weights(G.order, grid->dx);
+  cudaStream_t st = as_stream(stream);
+  if (ncomp == 1 && stream3d_ok(in, G, 1)) {
+    if (G.order == 2) return launch_stream3d<1, OP_GRAD, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
+    return launch_stream3d<2, OP_GRAD, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
+  }
+  const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp * G.ndims;
+  const int blocks = grid_blocks(total, 256);
+  if (G.order == 2) grad_generic_kernel<1><<<blocks, 256, 0, st>>>(in, out, G, ncomp, W, alpha, total);
+  else grad_generic_kernel<2><<<blocks, 256, 0, st>>>(in, out, G, ncomp, W, alpha, total);
+  return launch_status();
+}
+
+int pde_divergence(const float* in, float* out, const PdeGrid* grid, int32_t nrows, float alpha, void* stream) {
+  Geo G;
+  int rc = check_common(in, out, grid, nrows, &G);
+  if (rc) return rc;
+  const Weights W = d1_weights(G.order, grid->dx);
+  cudaStream_t st = as_stream(stream);
+  if (nrows == 1 && stream3d_ok(in, G, 3)) {
+    if (G.order == 2) return launch_stream3d<1, OP_DIV, 3, 64, 8, 2, 3>(in, out, G, W, alpha, st);
+    return launch_stream3d<2, OP_DIV, 3, 64, 8, 2, 3>(in, out, G, W, alpha, st);
+  }
+  const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * nrows;
+  const int blocks = grid_blocks(total, 256);
+  if (G.order == 2) div_generic_kernel<1><<<blocks, 256, 0, st>>>(in, out, G, nrows, W, alpha, total);
+  else div_generic_kernel<2><<<blocks, 256, 0, st>>>(in, out, G, nrows, W, alpha, total);
+  return launch_status();
+}
+
+int pde_euler(const float* y, const float* k, float dt, float* out, int64_t count, void* stream) {
+  if (!y || !k || !out || count < 0) return PDE_ERR_ARG;
+  if (count == 0) return PDE_OK;
+  cudaStream_t st = as_stream(stream);
+  int64_t n4 = 0;
+  if (aligned16(y) && aligned16(k) && aligned16(out)) {
+    n4 = count / 4;
+    if (n4 > 0)
+      euler_vec4_kernel<<<grid_blocks(n4, 256), 256, 0, st>>>(reinterpret_cast<const float4*>(y),
+                                                               reinterpret_cast<const float4*>(k), dt,
+                                                               reinterpret_cast<float4*>(out), n4);
+  }
+  if (4 * n4 < count)
+    euler_scalar_kernel<<<grid_blocks(count - 4 * n4, 256), 256, 0, st>>>(y, k, dt, out, 4 * n4, count);
+  return launch_status();
+}
+
+int pde_bc_apply(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, const PdeBCGroup* groups,
+                 int32_t ngroups, const float* t_device, void* stream) {
+  if (!in || !out || !grid || ncomp < 1 || ncomp > 32 || ngroups < 0 || (ngroups > 0 && !groups))
+    return PDE_ERR_ARG;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = (size_t)(G.n[0] * G.n[1] * G.n[2]) * ncomp * sizeof(float);
+  if (in != out) PDE_CUDA_CHECK(cudaMemcpyAsync(out, in, bytes, cudaMemcpyDeviceToDevice, st));
+  const float dx32 = (float)grid->dx;
+  for (int i = 0; i < ngroups; ++i) {
+    const PdeBCGroup& B = groups[i];
+    if (B.type != PDE_BC_DIRICHLET && B.type != PDE_BC_VON_NEUMANN) return PDE_ERR_ARG;
+    if (B.func != PDE_BC_FUNC_CONSTANT && B.func != PDE_BC_FUNC_RAMP) return PDE_ERR_ARG;
+    if (B.func == PDE_BC_FUNC_RAMP && !t_device) return PDE_ERR_ARG;
+    if (B.count < 0 || (B.count > 0 && !B.node_ids)) return PDE_ERR_ARG;
+    if (ncomp < 32 && (B.comp_mask >> ncomp) != 0) return PDE_ERR_ARG;
+    if (B.count == 0) continue;
+    bc_group_kernel<<<(B.count + 127) / 128, 128, 0, st>>>(in, out, G, ncomp, B.node_ids, B.count, B.type,
+                                                           B.comp_mask, B.func, B.value, B.t_max, t_device, dx32);
+  }
+  return launch_status();
+}
+
+int pde_periodic_fill(float* u, const PdeGrid* grid, int32_t ncomp, int32_t axis_mask, void* stream) {
+  if (!u || !grid || ncomp < 1) return PDE_ERR_ARG;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  if (G.g < 1) return PDE_ERR_GHOST;
+  cudaStream_t st = as_stream(stream);
+  for (int a = 0; a < 3; ++a) {
+    if (!((axis_mask >> a) & 1)) continue;
+    if (G.n[a] == 1) return PDE_ERR_ARG;
+    int64_t e[3] = {G.n[0], G.n[1], G.n[2]};
+    e[a] = 2 * G.g;
+    const int64_t total = e[0] * e[1] * e[2] * ncomp;
+    periodic_axis_kernel<<<grid_blocks(total, 256), 256, 0, st>>>(u, G, ncomp, a, total);
+  }
+  return launch_status();
+}
+
+int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* grid, int32_t ncomp,
+                   PdeBCRules* rules) {
+  if (!grid || !rules || ngroups < 0 || (ngroups > 0 && !groups)) return PDE_ERR_ARG;
+  if (ngroups > PDE_MAX_GROUPS) return PDE_ERR_TOO_LARGE;
+  if (ncomp < 1 || ncomp > PDE_FUSED_MAX_COMP) return PDE_ERR_UNSUPPORTED;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  if (G.g < 1) return PDE_ERR_GHOST;
+  memset(rules, 0, sizeof(*rules));
+  rules->ncomp = ncomp;
+  rules->ngroups = ngroups;
+  rules->dx32 = (float)grid->dx;
+  int elig_faces = 0;
+  for (int a = 0; a < 3; ++a)
+    if (G.n[a] > 1) elig_faces |= 3 << (2 * a);
+  for (int i = 0; i < ngroups; ++i) {
+    const PdeBCGroup& B = groups[i];
+    if (B.face_mask == 0) return PDE_ERR_UNSUPPORTED;
+    if (B.face_mask & ~elig_faces) return PDE_ERR_ARG;
+    if (B.type != PDE_BC_DIRICHLET && B.type != PDE_BC_VON_NEUMANN) return PDE_ERR_ARG;
+    if (B.func != PDE_BC_FUNC_CONSTANT && B.func != PDE_BC_FUNC_RAMP) return PDE_ERR_ARG;
+    if ((B.comp_mask >> ncomp) != 0) return PDE_ERR_ARG;
+    if (B.func == PDE_BC_FUNC_RAMP) rules->has_ramp = 1;
+    rules->group[i].type = B.type;
+    rules->group[i].comp_mask = B.comp_mask;
+    rules->group[i].func = B.func;
+    rules->group[i].value = B.value;
+    rules->group[i].t_max = B.t_max;
+  }
+  for (int K = 0; K < 27; ++K) {
+    const int k[3] = {K / 9, (K / 3) % 3, K % 3};
+    int faces = 0;
+    bool valid = true;
+    for (int a = 0; a < 3; ++a) {
+      if (G.n[a] == 1) {
+        if (k[a] != 1) valid = false;
+        continue;
+      }
+      if (k[a] == 0) faces |= 1 << (2 * a);
+      if (k[a] == 2) faces |= 1 << (2 * a + 1);
+    }
+    rules->node_group[K] = -1;
+    for (int a = 0; a < 3; ++a)
+      for (int v = 0; v < PDE_FUSED_MAX_COMP; ++v) rules->ghost_group[K][a][v] = -1;
+    if (!valid || faces == 0) continue;
+    for (int i = 0; i < ngroups; ++i) {
+      const PdeBCGroup& B = groups[i];
+      if (!(B.face_mask & faces)) continue;  // node not in this group
+      if (B.type == PDE_BC_DIRICHLET) rules->node_group[K] = (int8_t)i;
+      for (int a = 0; a < 3; ++a) {
+        if (G.n[a] == 1 || k[a] == 1) continue;  // no ghost along this axis
+        for (int v = 0; v < ncomp; ++v)
+          if ((B.comp_mask >> v) & 1u) rules->ghost_group[K][a][v] = (int8_t)i;
+      }
+    }
+  }
+  return PDE_OK;
+}
+
+int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
+                     const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
+                     void* stream) {
+  if (!u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
+  if (ncomp < 1 || ncomp > PDE_FUSED_MAX_COMP || rules->ncomp != ncomp) return PDE_ERR_ARG;
+  if (rules->has_ramp) return PDE_ERR_UNSUPPORTED;
+  if (work == u_in || work == u_out) return PDE_ERR_ARG;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  if (G.g < G.order / 2 || G.g < 1) return PDE_ERR_GHOST;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = (size_t)(G.n[0] * G.n[1] * G.n[2]) * ncomp * sizeof(float);
+  if (nsteps == 0) {
+    if (u_out != u_in) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, u_in, bytes, cudaMemcpyDeviceToDevice, st));
+    return PDE_OK;
+  }
+  const Weights W = lap_weights(G.order, grid->dx);
+  const int R = W.radius;
+  const bool two_d = (G.ndims == 2 && G.n[2] == 1);
+  int k = two_d ? (steps_per_pass > 0 ? steps_per_pass : 8) : 1;
+  if (k > nsteps) k = nsteps;
+  const int npasses = (nsteps + k - 1) / k;
+  // buffer sequence: the last pass writes u_out.
+  const float* src = u_in;
+  const bool alias = (u_out == u_in);
+  bool need_copy = false;
+  float* dst_first;
+  if (alias) {
+    dst_first = work;
+    need_copy = (npasses % 2) == 1;
+  } else {
+    dst_first = (npasses % 2 == 1) ? u_out : work;
+  }
+  float* dst = dst_first;
+  int done = 0;
+  for (int p = 0; p < npasses; ++p) {
+    const int ks = (nsteps - done < k) ? (nsteps - done) : k;
+    if (two_d) {
+      H2Params P;
+      P.X = (int)G.n[0]; P.Y = (int)G.n[1]; P.g = G.g; P.N = ncomp; P.k = ks;
+      P.TBX = 16; P.TBY = 32;
+      const int H = k * R;
+      P.RXM = P.TBX + 2 * H; P.RYM = P.TBY + 2 * H;
+      P.tiles_y = (P.Y + P.TBY - 1) / P.TBY;
+      const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+      for (int t = 0; t < 5; ++t) P.w[t] = W.w[t];
+      P.alpha = alpha; P.dt = dt;
+      const size_t smem = (size_t)2 * P.RXM * P.RYM * ncomp * sizeof(float);
+      if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+#define PDE_H2(RR, NN)                                                                                  \
+  do {                                                                                                  \
+    auto kern = heat2d_tb_kernel<RR, NN>;                                                               \
+    PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);                                                \
+  } while (0)
+      if (R == 1) {
+        switch (ncomp) {
+          case 1: PDE_H2(1, 1); break;
+          case 2: PDE_H2(1, 2); break;
+          case 3: PDE_H2(1, 3); break;
+          default: PDE_H2(1, 4); break;
+        }
+      } else {
+        switch (ncomp) {
+          case 1: PDE_H2(2, 1); break;
+          case 2: PDE_H2(2, 2); break;
+          case 3: PDE_H2(2, 3); break;
+          default: PDE_H2(2, 4); break;
+        }
+      }
+#undef PDE_H2
+    } else {
+      const int64_t total = G.n[0] * G.n[1] * G.n[2] * ncomp;
+      if (R == 1) heat_step_kernel<1><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, *rules, total);
+      else heat_step_kernel<2><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, *rules, total);
+    }
+    int rc = launch_status();
+    if (rc) return rc;
+    done += ks;
+    src = dst;
+    dst = (dst == work) ? u_out : work;
+  }
+  if (need_copy) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, work, bytes, cudaMemcpyDeviceToDevice, st));
+  return PDE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+"""The C-ABI library on CPU: it loads, exports every symbol the header
+declares, validates arguments without touching a GPU, and its host-side
+boundary-rule compiler reproduces the group-by-group semantics of the oracle."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import fdm
+from pde_module_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "pde_b200.h")
+
+
+def header_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pde_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_loads_and_exports_header_symbols():
+    L = _lib.lib()
+    syms = header_symbols()
+    assert len(syms) >= 11
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(_lib.exported_symbols()) >= set(syms)
+    assert L.pde_version() >= 100
+    assert L.pde_strerror(_lib.PDE_ERR_GHOST).decode().startswith("ghost")
+
+
+def test_argument_validation_needs_no_gpu():
+    L = _lib.lib()
+    g = _lib.make_grid((8, 8, 1), 1, 2, 0.1)
+    assert L.pde_laplacian(None, None, C.byref(g), 1, 1.0, None) == _lib.PDE_ERR_ARG
+    bad = _lib.make_grid((8, 8, 1), 0, 2, 0.1)
+    assert L.pde_laplacian(C.c_void_p(16), C.c_void_p(32), C.byref(bad), 1, 1.0, None) == _lib.PDE_ERR_GHOST
+    o3 = _lib.make_grid((8, 8, 1), 1, 3, 0.1)
+    assert L.pde_grad(C.c_void_p(16), C.c_void_p(32), C.byref(o3), 1, 1.0, None) == _lib.PDE_ERR_SHAPE
+    assert L.pde_euler(None, None, 0.1, None, 4, None) == _lib.PDE_ERR_ARG
+    r = _lib.PdeBCRules()
+    grp = (_lib.PdeBCGroup * 1)()
+    grp[0].type, grp[0].comp_mask, grp[0].face_mask = 1, 1, 0  # custom node list: not fusable
+    assert L.pde_bc_compile(grp, 1, C.byref(g), 1, C.byref(r)) == _lib.PDE_ERR_UNSUPPORTED
+
+
+# ---- rule compiler ----------------------------------------------------------
+def compile_rules(shape, g, ncomp, spec, dx=0.1):
+    """spec: (name, type, value, comps)"""
+    L = _lib.lib()
+    arr = (_lib.PdeBCGroup * len(spec))()
+    for i, (name, typ, val, comps) in enumerate(spec):
+        mask = 0
+        for c in comps:
+            mask |= 1 << c
+        fm = 0
+        if name == "ALL":
+            for a in range(3):
+                if shape[a] > 1:
+                    fm |= 3 << (2 * a)
+        else:
+            fm = _lib.FACE_BITS[name]
+        arr[i].type, arr[i].comp_mask, arr[i].func, arr[i].value, arr[i].face_mask = typ, mask, 0, val, fm
+    grid = _lib.make_grid(shape, g, 2, dx)
+    r = _lib.PdeBCRules()
+    assert L.pde_bc_compile(arr, len(spec), C.byref(grid), ncomp, C.byref(r)) == 0
+    return r
+
+
+def apply_rules(u, r, g, dx):
+    """NumPy model of the fused kernels' per-cell boundary evaluation (fused.cuh: bc_eval)."""
+    gs = u.shape[:3]
+    out = u.copy()
+    N = u.shape[3]
+
+    def cls(i, n, elig):
+        if not elig:
+            return 1
+        return 0 if i == g else (2 if i == n - 1 - g else 1)
+
+    for c in np.ndindex(*gs):
+        ghost_axes, deep = [], False
+        for a in range(3):
+            if gs[a] == 1:
+                continue
+            if c[a] < g or c[a] > gs[a] - 1 - g:
+                if c[a] in (g - 1, gs[a] - g):
+                    ghost_axes.append(a)
+                else:
+                    deep = True
+        for v in range(N):
+            if deep or len(ghost_axes) > 1:
+                continue
+            if ghost_axes:
+                a = ghost_axes[0]
+                inc = 1 if c[a] == g - 1 else -1
+                p = list(c)
+                p[a] += inc
+                K = cls(p[0], gs[0], gs[0] > 1) * 9 + cls(p[1], gs[1], gs[1] > 1) * 3 + cls(p[2], gs[2], gs[2] > 1)
+                gi = r.ghost_group[K][a][v]
+                if gi < 0:
+                    continue
+                p[a] += inc
+                G = r.group[gi]
+                a_val = u[tuple(p) + (v,)]
+                val = np.float32(G.value)
+                if G.type == 1:
+                    out[c + (v,)] = np.float32(2.0) * val - a_val
+                else:
+                    out[c + (v,)] = (np.float32(-2 * inc) * np.float32(r.dx32)) * val + a_val
+            else:
+                K = cls(c[0], gs[0], gs[0] > 1) * 9 + cls(c[1], gs[1], gs[1] > 1) * 3 + cls(c[2], gs[2], gs[2] > 1)
+                if K == 13:
+                    continue
+                gi = r.node_group[K]
+                if gi >= 0 and (r.group[gi].comp_mask >> v) & 1:
+                    out[c + (v,)] = np.float32(r.group[gi].value)
+    return out
+
+
+SPECS = [
+    ((9, 8, 1), 1, 1, [("ALL", 1, 0.0, (0,))]),
+    ((9, 8, 1), 1, 2, [("ALL", 1, 0.0, (0, 1)), ("+Y", 1, 1.0, (0,))]),
+    ((9, 8, 1), 1, 1, [("ALL", 2, 0.0, (0,))]),
+    ((9, 8, 1), 2, 2, [("-X", 2, 0.5, (0, 1)), ("-X", 1, 0.0, (0,)), ("+Y", 2, -1.5, (1,))]),
+    ((7, 6, 5), 1, 3, [("ALL", 1, 0.0, (0, 1, 2)), ("+Z", 1, 2.0, (2,)), ("-Y", 2, 0.25, (0,))]),
+    ((6, 7, 8), 1, 1, [("-X", 1, 1.0, (0,)), ("+X", 1, -1.0, (0,)), ("ALL", 2, 0.0, (0,))]),
+]
+
+
+@pytest.mark.parametrize("shape,g,N,spec", SPECS)
+def test_compiled_rules_match_group_semantics(shape, g, N, spec):
+    rng = np.random.default_rng(7)
+    dx = 0.1
+    u = rng.standard_normal(shape + (N,)).astype(np.float32)
+    groups = fdm.standard_groups(shape, g, spec)
+    ref = fdm.bc_apply(u, groups, dx, g)
+    r = compile_rules(shape, g, N, spec, dx)
+    got = apply_rules(u, r, g, dx)
+    np.testing.assert_array_equal(got, ref)
