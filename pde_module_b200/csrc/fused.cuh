@@ -197,16 +197,18 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
 }
 
 // k fused steps on a 2D grid (X, Y, 1, N) per pass.  Tiles cover the whole
-// array (ghosts included); the smem region is the tile grown by k*R cells on
-// each side (clipped to the array).  After k sub-steps the tile itself is
-// exact: garbage enters only from the region's cut edges, R cells per step.
+// array (ghosts included); the smem region is the tile grown by H = k*R + 1
+// cells on each side (clipped to the array).  Values invalidated by the
+// region's cut edges move inward R cells per step; the extra cell covers the
+// output ghost cells, whose last boundary fill reads the cell two steps
+// inward (adj) at the previous step.
 template <int R, int N>
 __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                         const H2Params P, const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];
   const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
   const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
-  const int H = P.k * R;
+  const int H = P.k * R + 1;
   const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, P.X);
   const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
   const int RX = rx1 - rx0, RY = ry1 - ry0;

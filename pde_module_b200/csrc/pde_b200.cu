@@ -339,7 +339,7 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
       H2Params P;
       P.X = (int)G.n[0]; P.Y = (int)G.n[1]; P.g = G.g; P.N = ncomp; P.k = ks;
       P.TBX = 16; P.TBY = 32;
-      const int H = k * R;
+      const int H = k * R + 1;  // must match heat2d_tb_kernel
       P.RXM = P.TBX + 2 * H; P.RYM = P.TBY + 2 * H;
       P.tiles_y = (P.Y + P.TBY - 1) / P.TBY;
       const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;

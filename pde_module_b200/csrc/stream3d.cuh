@@ -37,10 +37,12 @@ struct S3Cfg {
   static constexpr int TYG = TY / YPT;
   static constexpr int THREADS = LANES * TYG;
   static constexpr int ROWS = TY + 2 * R;
-  static constexpr int W = round4(3 + (TZ + 2 * R) * CIN);
+  static constexpr int W = round4(3 + (TZ + 2 * R) * CIN);  // TMA box (floats)
+  static constexpr int WP = (W + 31) & ~31;  // smem row pitch: TMA destinations are 128-byte aligned
   static constexpr int S = 2 * R + 1 + PREF;
-  static constexpr int STAGE_FLOATS = ROWS * W;
-  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)S * 8;
+  static constexpr int STAGE_FLOATS = ROWS * WP;
+  // + 128: the base is rounded up to a 128-byte boundary at run time
+  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)S * 8 + 128;
   static_assert(ROWS <= 32, "one warp issues the row copies of a stage");
   static_assert(W <= 256, "TMA box extent");
   static_assert(TY % YPT == 0, "rows per thread");
@@ -50,8 +52,9 @@ template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
 __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS)
     stream3d_kernel(const __grid_constant__ CUtensorMap tmap, const S3Params P) {
   using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>;
-  constexpr int ROWS = C::ROWS, W = C::W, S = C::S, T = 2 * R + 1;
-  extern __shared__ __align__(128) float smem[];
+  constexpr int ROWS = C::ROWS, W = C::W, WP = C::WP, S = C::S, T = 2 * R + 1;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* smem = reinterpret_cast<float*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_FLOATS);
 
   int bid = blockIdx.x;
@@ -85,7 +88,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS)
     if (wl < ROWS) {
       const int y = y0 - R + wl;
       const int f0 = (x * P.Y + y) * P.Z * CIN + zc;
-      tma_load_1d(smem + (s * ROWS + wl) * W, &tmap, f0 & ~3, &bar[s]);
+      tma_load_1d(smem + (s * ROWS + wl) * WP, &tmap, f0 & ~3, &bar[s]);
     }
   };
   bool dead = false;
@@ -130,7 +133,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS)
 #pragma unroll
     for (int k = 0; k < YPT; ++k) {
       const int r = R + yg * YPT + k;
-      q[i + 1][k] = sp[r * W + lead(x, y0 - R + r) + cofs + qc];
+      q[i + 1][k] = sp[r * WP + lead(x, y0 - R + r) + cofs + qc];
     }
   }
 
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS)
 #pragma unroll
       for (int k = 0; k < YPT; ++k) {
         const int r = R + yg * YPT + k;
-        q[T - 1][k] = sp[r * W + lead(x, y0 - R + r) + cofs + qc];
+        q[T - 1][k] = sp[r * WP + lead(x, y0 - R + r) + cofs + qc];
       }
     }
     const float* sc = stage(j + R);
@@ -161,13 +164,13 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS)
 #pragma unroll
     for (int m = 0; m < YPT + 2 * R; ++m) {
       const int r = yg * YPT + m;
-      col[m] = sc[r * W + lead(xc, y0 - R + r) + cofs + yc];
+      col[m] = sc[r * WP + lead(xc, y0 - R + r) + cofs + yc];
     }
 #pragma unroll
     for (int k = 0; k < YPT; ++k) {
       const int r = R + yg * YPT + k;
       const int yk = y0 - R + r;
-      const float* rowp = sc + r * W + lead(xc, yk) + cofs + zcmp;
+      const float* rowp = sc + r * WP + lead(xc, yk) + cofs + zcmp;
       if constexpr (OP == OP_LAP || OP == OP_DIV) {
         float acc = 0.0f;
 #pragma unroll
