@@ -149,6 +149,23 @@ int pde_grad(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
 int pde_divergence(const float* in, float* out, const PdeGrid* grid, int32_t nrows,
                    float alpha, void* stream);
 
+/* Arithmetic modes of the _ex operator variants.  PDE_MODE_EXACT (what the
+ * plain entry points use) rounds every product and sum of the reference's sum
+ * separately, in its order: results are bit-identical to the reference
+ * algorithm.  PDE_MODE_FAST sums taps that share a weight before multiplying,
+ * folds alpha into the weights and uses FMA (3D streaming kernels; other
+ * shapes run the exact kernels).  Its results differ from exact ones by a few
+ * float32 roundings of the summed terms (relative L2 difference ~1e-7 on
+ * random fields) and a zero-weight tap no longer propagates NaN/Inf. */
+#define PDE_MODE_EXACT 0
+#define PDE_MODE_FAST  1
+int pde_laplacian_ex(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha,
+                     int32_t mode, void* stream);
+int pde_grad_ex(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, int32_t mode,
+                void* stream);
+int pde_divergence_ex(const float* in, float* out, const PdeGrid* grid, int32_t nrows, float alpha,
+                      int32_t mode, void* stream);
+
 /* out[i] = y[i] + dt * k[i] for i < count (floats), time_step/forwardEuler.py:70-79. */
 int pde_euler(const float* y, const float* k, float dt, float* out, int64_t count,
               void* stream);

@@ -12,7 +12,11 @@ import ctypes as C
 
 import torch
 
-from ..._lib import lib, check, stream_ptr, require_cuda_f32
+from ..._lib import lib, check, stream_ptr, require_cuda_f32, PDE_MODE_EXACT, PDE_MODE_FAST
+
+
+def _mode(kernel) -> int:
+    return PDE_MODE_FAST if getattr(kernel, "fast", False) else PDE_MODE_EXACT
 
 
 def _check_io(kernel, input_array, output_array, in_trailing, out_trailing):
@@ -35,8 +39,8 @@ def laplacian(kernel, input_array: torch.Tensor, alpha: float, output_array: tor
     if ghost_cells != kernel.ghost_cells:
         raise AssertionError("ghost_cells differs from the kernel's")
     _check_io(kernel, input_array, output_array, (kernel.ncomp,), (kernel.ncomp,))
-    check(lib().pde_laplacian(C.c_void_p(input_array.data_ptr()), C.c_void_p(output_array.data_ptr()),
-                              C.byref(kernel.grid), kernel.ncomp, float(alpha),
+    check(lib().pde_laplacian_ex(C.c_void_p(input_array.data_ptr()), C.c_void_p(output_array.data_ptr()),
+                              C.byref(kernel.grid), kernel.ncomp, float(alpha), _mode(kernel),
                               C.c_void_p(stream_ptr(input_array))), "pde_laplacian")
     return output_array
 
@@ -50,8 +54,8 @@ def grad(kernel, input_array: torch.Tensor, alpha: float, output_array: torch.Te
     if out_tr not in ((kernel.ncomp, D),) and not (kernel.ncomp == 1 and out_tr == (D,)):
         raise AssertionError(f"grad output components {out_tr} do not match ({kernel.ncomp}, {D})")
     _check_io(kernel, input_array, output_array, (kernel.ncomp,), out_tr)
-    check(lib().pde_grad(C.c_void_p(input_array.data_ptr()), C.c_void_p(output_array.data_ptr()),
-                         C.byref(kernel.grid), kernel.ncomp, float(alpha),
+    check(lib().pde_grad_ex(C.c_void_p(input_array.data_ptr()), C.c_void_p(output_array.data_ptr()),
+                         C.byref(kernel.grid), kernel.ncomp, float(alpha), _mode(kernel),
                          C.c_void_p(stream_ptr(input_array))), "pde_grad")
     return output_array
 
@@ -65,7 +69,7 @@ def divergence(kernel, input_array: torch.Tensor, alpha: float, ghost_cells: int
     if in_tr not in ((kernel.ncomp, D),) and not (kernel.ncomp == 1 and in_tr == (D,)):
         raise AssertionError(f"divergence input components {in_tr} do not match ({kernel.ncomp}, {D})")
     _check_io(kernel, input_array, output_array, in_tr, (kernel.ncomp,))
-    check(lib().pde_divergence(C.c_void_p(input_array.data_ptr()), C.c_void_p(output_array.data_ptr()),
-                               C.byref(kernel.grid), kernel.ncomp, float(alpha),
+    check(lib().pde_divergence_ex(C.c_void_p(input_array.data_ptr()), C.c_void_p(output_array.data_ptr()),
+                               C.byref(kernel.grid), kernel.ncomp, float(alpha), _mode(kernel),
                                C.c_void_p(stream_ptr(input_array))), "pde_divergence")
     return output_array

@@ -22,6 +22,7 @@ class StencilPlan:
     dx: float
     ncomp: int              # N of the input vector (rows of a matrix input)
     dimension: int          # number of eligible axes
+    fast: bool = False      # PDE_MODE_FAST arithmetic (see include/pde_b200.h)
     grid: PdeGrid = field(repr=False, default=None)
 
     def __post_init__(self):
@@ -32,19 +33,22 @@ class StencilPlan:
         self.grid = make_grid(self.grid_shape, self.ghost_cells, self.order, self.dx)
 
 
-def _plan(op, ncomp, grid_shape, dx, ghost_cells, order):
+def _plan(op, ncomp, grid_shape, dx, ghost_cells, order, fast):
     gs = _types.grid_shape_of(grid_shape)
     return StencilPlan(op, gs, int(ghost_cells), int(order), float(dx), int(ncomp),
-                       _types.dimension_of(gs))
+                       _types.dimension_of(gs), bool(fast))
 
 
-def create_Laplacian_kernel(ncomp: int, grid_shape, dx: float, ghost_cells: int, order: int = 2) -> StencilPlan:
-    return _plan("laplacian", ncomp, grid_shape, dx, ghost_cells, order)
+def create_Laplacian_kernel(ncomp: int, grid_shape, dx: float, ghost_cells: int, order: int = 2,
+                            fast: bool = False) -> StencilPlan:
+    return _plan("laplacian", ncomp, grid_shape, dx, ghost_cells, order, fast)
 
 
-def create_Grad_kernel(ncomp: int, grid_shape, dx: float, ghost_cells: int, order: int = 2) -> StencilPlan:
-    return _plan("grad", ncomp, grid_shape, dx, ghost_cells, order)
+def create_Grad_kernel(ncomp: int, grid_shape, dx: float, ghost_cells: int, order: int = 2,
+                       fast: bool = False) -> StencilPlan:
+    return _plan("grad", ncomp, grid_shape, dx, ghost_cells, order, fast)
 
 
-def create_Divergence_kernel(nrows: int, grid_shape, dx: float, ghost_cells: int, order: int = 2) -> StencilPlan:
-    return _plan("divergence", nrows, grid_shape, dx, ghost_cells, order)
+def create_Divergence_kernel(nrows: int, grid_shape, dx: float, ghost_cells: int, order: int = 2,
+                             fast: bool = False) -> StencilPlan:
+    return _plan("divergence", nrows, grid_shape, dx, ghost_cells, order, fast)

@@ -21,9 +21,10 @@ class Divergence(ExplicitUniformGridStencil):
     """
 
     def __init__(self, inputs, grid_shape, dx: float, ghost_cells: int, stencil=None,
-                 float_dtype=torch.float32, order: int = 2) -> None:
+                 float_dtype=torch.float32, order: int = 2, fast: bool = False) -> None:
         if stencil is not None:
             raise ValueError("Custom stencil not implemented yet")
+        self.fast = bool(fast)
         dimension = self.calculate_dimension_from_grid_shape(grid_shape)
         is_vector = False
         if isinstance(inputs, Iterable):
@@ -49,7 +50,8 @@ class Divergence(ExplicitUniformGridStencil):
     @setup
     def initialize_kernel(self, input_array: torch.Tensor, *args, **kwargs) -> None:
         self.kernel = create_Divergence_kernel(self.outputs[0], input_array.shape, self.dx_value,
-                                               self.ghost_cells, self.order)
+                                               self.ghost_cells, self.order,
+                                              fast=self.fast)
         self.kernel_dim = self.grid_shape_with_no_ghost_cells(input_array.shape, self.ghost_cells)
 
     def forward(self, input_array: torch.Tensor, alpha: float = 1.0, *args, **kwargs) -> torch.Tensor:

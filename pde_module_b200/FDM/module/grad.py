@@ -17,9 +17,10 @@ class Grad(ExplicitUniformGridStencil):
     """
 
     def __init__(self, inputs: int, grid_shape, dx: float, ghost_cells: int, stencil=None,
-                 force_matrix: bool = False, float_dtype=torch.float32, order: int = 2) -> None:
+                 force_matrix: bool = False, float_dtype=torch.float32, order: int = 2, fast: bool = False) -> None:
         if stencil is not None:
             raise ValueError("Custom stencil not implemented yet")
+        self.fast = bool(fast)
         self.force_matrix = force_matrix
         dimension = self.calculate_dimension_from_grid_shape(grid_shape)
         assert type(inputs) is int and inputs > 0
@@ -31,7 +32,7 @@ class Grad(ExplicitUniformGridStencil):
     def initialize_kernel(self, input_array: torch.Tensor, *args, **kwargs) -> None:
         assert len(self.inputs) == 1, "Grad Only For Vectors"
         self.kernel = create_Grad_kernel(self.inputs[0], input_array.shape, self.dx_value, self.ghost_cells,
-                                         self.order)
+                                         self.order, fast=self.fast)
         assert self.kernel.dimension == (self.outputs[-1]), "grid dimension differs from the constructor's"
         self.kernel_dim = self.grid_shape_with_no_ghost_cells(input_array.shape, self.ghost_cells)
 

@@ -19,16 +19,18 @@ class Laplacian(ExplicitUniformGridStencil):
     """
 
     def __init__(self, inputs: int, dx: float, ghost_cells: int, stencil=None, float_dtype=torch.float32,
-                 order: int = 2) -> None:
+                 order: int = 2, fast: bool = False) -> None:
         if stencil is not None:
             raise ValueError("Custom stencil not implemented yet")
+        self.fast = bool(fast)
         super().__init__(inputs, inputs, dx, ghost_cells, float_dtype=float_dtype, order=order)
 
     @setup
     def initialize_kernel(self, input_array: torch.Tensor, *args, **kwargs) -> None:
         assert len(self.inputs) == 1, "Laplacian Only For Vectors"
         self.kernel = create_Laplacian_kernel(self.inputs[0], input_array.shape, self.dx_value,
-                                              self.ghost_cells, self.order)
+                                              self.ghost_cells, self.order,
+                                              fast=self.fast)
         self.kernel_dim = self.grid_shape_with_no_ghost_cells(input_array.shape, self.ghost_cells)
 
     def forward(self, input_array: torch.Tensor, alpha: float = 1.0, *args, **kwargs) -> torch.Tensor:

@@ -25,6 +25,10 @@ PDE_ERR_UNSUPPORTED = -6
 PDE_ERR_TIMEOUT = -7
 PDE_ERR_TOO_LARGE = -8
 
+PDE_MODE_EXACT = 0
+PDE_MODE_FAST = 1
+PDE_DISPATCH_AUTO = 0
+PDE_DISPATCH_GENERIC = 1
 PDE_BC_DIRICHLET = 1
 PDE_BC_VON_NEUMANN = 2
 PDE_BC_FUNC_CONSTANT = 0
@@ -77,6 +81,12 @@ _SIGS = {
     "pde_laplacian": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_void_p]),
     "pde_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_void_p]),
     "pde_divergence": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_void_p]),
+    "pde_laplacian_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_int32,
+                                   C.c_void_p]),
+    "pde_grad_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_int32,
+                              C.c_void_p]),
+    "pde_divergence_ex": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_int32,
+                                    C.c_void_p]),
     "pde_euler": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int64, C.c_void_p]),
     "pde_bc_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.POINTER(PdeBCGroup),
                                C.c_int32, C.c_void_p, C.c_void_p]),

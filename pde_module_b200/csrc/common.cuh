@@ -21,6 +21,7 @@ struct Geo {
 // Stencil weights rounded to fp32, largest stencil is 5 taps.
 struct Weights {
   float w[5];
+  double wd[5];  // the same weights before rounding to fp32
   int taps;  // 3 or 5
   int radius;
 };
@@ -61,13 +62,13 @@ inline Weights lap_weights(int order, double dx) {
   if (order == 2) {
     double d2 = dx * dx;
     W.taps = 3; W.radius = 1;
-    W.w[0] = (float)(1.0 / d2); W.w[1] = (float)(-2.0 / d2); W.w[2] = (float)(1.0 / d2);
+    W.wd[0] = 1.0 / d2; W.wd[1] = -2.0 / d2; W.wd[2] = 1.0 / d2;
   } else {
     double d = 12.0 * dx * dx;
     W.taps = 5; W.radius = 2;
-    W.w[0] = (float)(-1.0 / d); W.w[1] = (float)(16.0 / d); W.w[2] = (float)(-30.0 / d);
-    W.w[3] = (float)(16.0 / d); W.w[4] = (float)(-1.0 / d);
+    W.wd[0] = -1.0 / d; W.wd[1] = 16.0 / d; W.wd[2] = -30.0 / d; W.wd[3] = 16.0 / d; W.wd[4] = -1.0 / d;
   }
+  for (int t = 0; t < W.taps; ++t) W.w[t] = (float)W.wd[t];
   return W;
 }
 
@@ -77,13 +78,13 @@ inline Weights d1_weights(int order, double dx) {
   Weights W{};
   if (order == 2) {
     W.taps = 3; W.radius = 1;
-    W.w[0] = (float)(-1.0 / (2 * dx)); W.w[1] = 0.0f; W.w[2] = (float)(1.0 / (2 * dx));
+    W.wd[0] = -1.0 / (2 * dx); W.wd[1] = 0.0; W.wd[2] = 1.0 / (2 * dx);
   } else {
     double d = 12.0 * dx;
     W.taps = 5; W.radius = 2;
-    W.w[0] = (float)(1.0 / d); W.w[1] = (float)(-8.0 / d); W.w[2] = 0.0f;
-    W.w[3] = (float)(8.0 / d); W.w[4] = (float)(-1.0 / d);
+    W.wd[0] = 1.0 / d; W.wd[1] = -8.0 / d; W.wd[2] = 0.0; W.wd[3] = 8.0 / d; W.wd[4] = -1.0 / d;
   }
+  for (int t = 0; t < W.taps; ++t) W.w[t] = (float)W.wd[t];
   return W;
 }
 
@@ -92,6 +93,28 @@ inline Weights d1_weights(int order, double dx) {
 __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+
+// Packed pairs of fp32 (sm_100 f32x2 arithmetic): each lane is one IEEE
+// round-to-nearest operation, exactly like the scalar mul/add above.
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pack2(float a, float b) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void unpack2(f2 r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
 
 inline int grid_blocks(int64_t work, int threads, int64_t cap = 148LL * 64) {
   int64_t b = (work + threads - 1) / threads;

@@ -31,10 +31,11 @@ int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ER
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // ---- 3D streaming dispatch -------------------------------------------------
-template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
-int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt, float alpha, cudaStream_t st) {
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, bool PP0, int MODE>
+int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& Wt, double alpha_d, float alpha,
+                      cudaStream_t st) {
   using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>;
-  auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF>;
+  auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF, PP0, MODE>;
   static int occ = -1;
   if (occ < 0) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM) != cudaSuccess)
@@ -54,18 +55,56 @@ int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt
   for (int t = 0; t < 5; ++t) P.w[t] = Wt.w[t];
   P.alpha = alpha;
   P.out = out;
-  const int tiles = P.ny_tiles * P.nz_tiles;
-  const int resident = occ * sm_count();
-  int nchunks = resident / tiles;
-  if (nchunks < 1) nchunks = 1;
+  // Persistent grid over (chunk, tile) items in chunk-major order.  The chunk
+  // count is chosen by a load model: the busiest SM runs ceil(blocks/SMs)
+  // blocks of ceil(items/blocks) items each, against the ideal items/SMs, and
+  // each item re-reads 2R planes at its ends.
+  P.ntiles = P.ny_tiles * P.nz_tiles;
   const int nx = (int)G.ext[0];
-  if (nchunks > nx) nchunks = nx;
-  P.chunk = (nx + nchunks - 1) / nchunks;
-  nchunks = (nx + P.chunk - 1) / P.chunk;
+  const int sms = sm_count();
+  const long long slots = (long long)occ * sms;
+  int best_n = 1;
+  double best = -1.0;
+  for (int n = 1; n <= 64 && n <= nx; ++n) {
+    const int ch = (nx + n - 1) / n;
+    const int nn = (nx + ch - 1) / ch;
+    const long long items = (long long)P.ntiles * nn;
+    const long long B = items < slots ? items : slots;
+    const long long per_block = (items + B - 1) / B;
+    const long long per_sm = (B + sms - 1) / sms;
+    const double eff = ((double)items / sms) / (double)(per_block * per_sm) * (double)ch / (ch + R);
+    if (eff > best + 1e-9) { best = eff; best_n = n; }
+  }
+  P.chunk = (nx + best_n - 1) / best_n;
+  const int nchunks = (nx + P.chunk - 1) / P.chunk;
+  P.nitems = P.ntiles * nchunks;
+  long long blocks = slots < P.nitems ? slots : P.nitems;
   CUtensorMap m;
   if (!encode_1d(&m, in, (uint64_t)total, (uint32_t)C::W)) return PDE_ERR_CUDA;
-  kern<<<tiles * nchunks, dim3(C::LANES, C::TYG), C::SMEM, st>>>(m, P);
+  FastW FW{};
+  if (MODE == MODE_FAST) {
+    // folded weights from the double-precision stencil (Weights::wd)
+    if (OP == OP_LAP) {
+      for (int t = 0; t < R; ++t) FW.a[t] = (float)(alpha_d * Wt.wd[t]);
+      FW.a[R] = (float)(alpha_d * 3.0 * Wt.wd[R]);
+    } else {
+      for (int t = R + 1; t < 2 * R + 1; ++t) FW.a[t - R - 1] = (float)(alpha_d * Wt.wd[t]);
+    }
+  }
+  kern<<<(unsigned)blocks, C::THREADS, C::SMEM, st>>>(m, P, FW);
   return launch_status();
+}
+
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
+int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt, float alpha, int mode,
+                    cudaStream_t st) {
+  const bool pp0 = ((G.n[1] * G.n[2] * CIN) & 3) == 0;
+  if (mode == PDE_MODE_FAST) {
+    if (pp0) return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, true, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
+    return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, false, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
+  }
+  if (pp0) return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, true, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
+  return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, false, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
 }
 
 // The flat 1D TMA view addresses floats with int32 coordinates, including rows
@@ -126,6 +165,12 @@ int pde_device_error(void* stream) {
 }
 
 int pde_laplacian(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, void* stream) {
+  return pde_laplacian_ex(in, out, grid, ncomp, alpha, PDE_MODE_EXACT, stream);
+}
+
+int pde_laplacian_ex(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, int32_t mode,
+                     void* stream) {
+  if (mode != PDE_MODE_EXACT && mode != PDE_MODE_FAST) return PDE_ERR_ARG;
   Geo G;
   int rc = check_common(in, out, grid, ncomp, &G);
   if (rc) return rc;
@@ -133,11 +178,11 @@ int pde_laplacian(const float* in, float* out, const PdeGrid* grid, int32_t ncom
   cudaStream_t st = as_stream(stream);
   if ((ncomp == 1 || ncomp == 3) && stream3d_ok(in, G, ncomp)) {
     if (G.order == 2) {
-      if (ncomp == 1) return launch_stream3d<1, OP_LAP, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
-      return launch_stream3d<1, OP_LAP, 3, 32, 16, 4, 3>(in, out, G, W, alpha, st);
+      if (ncomp == 1) return launch_stream3d<1, OP_LAP, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
+      return launch_stream3d<1, OP_LAP, 3, 32, 16, 8, 4>(in, out, G, W, alpha, mode, st);
     } else {
-      if (ncomp == 1) return launch_stream3d<2, OP_LAP, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
-      return launch_stream3d<2, OP_LAP, 3, 32, 16, 4, 3>(in, out, G, W, alpha, st);
+      if (ncomp == 1) return launch_stream3d<2, OP_LAP, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
+      return launch_stream3d<2, OP_LAP, 3, 32, 16, 8, 4>(in, out, G, W, alpha, mode, st);
     }
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp;
@@ -148,14 +193,20 @@ int pde_laplacian(const float* in, float* out, const PdeGrid* grid, int32_t ncom
 }
 
 int pde_grad(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, void* stream) {
+  return pde_grad_ex(in, out, grid, ncomp, alpha, PDE_MODE_EXACT, stream);
+}
+
+int pde_grad_ex(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, float alpha, int32_t mode,
+                void* stream) {
+  if (mode != PDE_MODE_EXACT && mode != PDE_MODE_FAST) return PDE_ERR_ARG;
   Geo G;
   int rc = check_common(in, out, grid, ncomp, &G);
   if (rc) return rc;
   const Weights W = d1_weights(G.order, grid->dx);
   cudaStream_t st = as_stream(stream);
   if (ncomp == 1 && stream3d_ok(in, G, 1)) {
-    if (G.order == 2) return launch_stream3d<1, OP_GRAD, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
-    return launch_stream3d<2, OP_GRAD, 1, 64, 16, 4, 3>(in, out, G, W, alpha, st);
+    if (G.order == 2) return launch_stream3d<1, OP_GRAD, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
+    return launch_stream3d<2, OP_GRAD, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp * G.ndims;
   const int blocks = grid_blocks(total, 256);
@@ -165,14 +216,20 @@ int pde_grad(const float* in, float* out, const PdeGrid* grid, int32_t ncomp, fl
 }
 
 int pde_divergence(const float* in, float* out, const PdeGrid* grid, int32_t nrows, float alpha, void* stream) {
+  return pde_divergence_ex(in, out, grid, nrows, alpha, PDE_MODE_EXACT, stream);
+}
+
+int pde_divergence_ex(const float* in, float* out, const PdeGrid* grid, int32_t nrows, float alpha, int32_t mode,
+                      void* stream) {
+  if (mode != PDE_MODE_EXACT && mode != PDE_MODE_FAST) return PDE_ERR_ARG;
   Geo G;
   int rc = check_common(in, out, grid, nrows, &G);
   if (rc) return rc;
   const Weights W = d1_weights(G.order, grid->dx);
   cudaStream_t st = as_stream(stream);
   if (nrows == 1 && stream3d_ok(in, G, 3)) {
-    if (G.order == 2) return launch_stream3d<1, OP_DIV, 3, 64, 8, 2, 3>(in, out, G, W, alpha, st);
-    return launch_stream3d<2, OP_DIV, 3, 64, 8, 2, 3>(in, out, G, W, alpha, st);
+    if (G.order == 2) return launch_stream3d<1, OP_DIV, 3, 64, 16, 8, 2>(in, out, G, W, alpha, mode, st);
+    return launch_stream3d<2, OP_DIV, 3, 64, 16, 8, 2>(in, out, G, W, alpha, mode, st);
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * nrows;
   const int blocks = grid_blocks(total, 256);

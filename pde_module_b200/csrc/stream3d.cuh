@@ -1,19 +1,26 @@
 // 2.5D streaming stencils for 3D grids with TMA-staged halo tiles.
 //
 // A block owns a (TY x TZ) tile of interior (y, z) columns and marches along
-// X (the slowest axis) over a chunk of planes.  Each input plane of the tile
-// (TY + 2R rows, each TZ + 2R cells plus alignment lead) is brought into a
-// ring of S shared-memory stages by 1D TMA bulk-tensor copies (one per row:
-// the array's row pitch is arbitrary, e.g. 514 floats, so a 3D tensor map's
-// 16-byte stride rule cannot be met) completing on one mbarrier per stage.
-// Loads run S - 2R - 1 planes ahead of the plane being computed.  X-direction
-// taps come from a register queue of the thread's own column; Y and Z taps
-// come from the centre stage.  Every product and sum is rounded separately,
-// in the reference's order (axes ascending, taps low to high, alpha last), so
-// the results are bit-identical to the general kernels.
+// X (the slowest axis) over a chunk of planes.  One producer warp brings each
+// input plane of the tile (TY + 2R rows of TZ + 2R cells plus an alignment
+// lead) into a ring of S shared-memory stages with 1D TMA bulk-tensor copies,
+// one per row: the array's row pitch is arbitrary (e.g. 514 floats), so a 3D
+// tensor map's 16-byte stride rule cannot be met.  Each stage has a "full"
+// mbarrier (TMA bytes landed) and an "empty" mbarrier (every consumer warp is
+// done with the plane); there is no block-wide barrier in the plane loop.
+//
+// Consumer threads own a z column and YPT consecutive rows.  X-direction taps
+// come from a register queue of the thread's own column (a plane's centre
+// values are read once, when the plane arrives); Y and Z taps come from the
+// centre plane's stage, which is released right after use, so a stage is
+// held only while its plane is the centre or newest plane.  Every product and
+// sum is rounded separately, in the reference's order (axes ascending, taps
+// low to high, alpha last): results equal the general kernels' bit for bit,
+// up to the sign of an exactly-zero result (the leading 0 + w*u is skipped).
 #pragma once
 #include "common.cuh"
 #include "tma.cuh"
+#include <type_traits>
 
 namespace pde {
 
@@ -21,8 +28,9 @@ enum { OP_LAP = 0, OP_GRAD = 1, OP_DIV = 2 };
 
 struct S3Params {
   int X, Y, Z, g;
-  int chunk;            // output planes per block
-  int ny_tiles, nz_tiles;
+  int ny_tiles, nz_tiles, ntiles;
+  int chunk;            // planes per work item
+  int nitems;           // ntiles x chunks, chunk-major
   int pp, pr;           // (Y*Z*CIN) mod 4, (Z*CIN) mod 4: row alignment lead
   float w[5];
   float alpha;
@@ -31,182 +39,303 @@ struct S3Params {
 
 __host__ __device__ constexpr int round4(int v) { return (v + 3) & ~3; }
 
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < N) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, N>(f);
+  }
+}
+
 template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
 struct S3Cfg {
-  static constexpr int LANES = (OP == OP_LAP) ? TZ * CIN : TZ;
-  static constexpr int TYG = TY / YPT;
-  static constexpr int THREADS = LANES * TYG;
+  static constexpr int LANES = (OP == OP_LAP) ? TZ * CIN : TZ;  // consumer threads per row group
+  static constexpr int TYG = TY / YPT;                           // row groups
+  static constexpr int NCONS = LANES * TYG;                      // consumer threads
+  static constexpr int NCW = NCONS / 32;                         // consumer warps
+  static constexpr int THREADS = NCONS + 32;                     // + one producer warp
   static constexpr int ROWS = TY + 2 * R;
   static constexpr int W = round4(3 + (TZ + 2 * R) * CIN);  // TMA box (floats)
-  static constexpr int WP = (W + 31) & ~31;  // smem row pitch: TMA destinations are 128-byte aligned
-  static constexpr int S = 2 * R + 1 + PREF;
+  static constexpr int WP = (W + 31) & ~31;                 // smem row pitch: 128-byte aligned rows
+  static constexpr int S = R + 1 + PREF;                    // stages: centre .. newest + prefetch
   static constexpr int STAGE_FLOATS = ROWS * WP;
   // + 128: the base is rounded up to a 128-byte boundary at run time
-  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)S * 8 + 128;
-  static_assert(ROWS <= 32, "one warp issues the row copies of a stage");
+  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)2 * S * 8 + 128;
+  static_assert(NCONS % 32 == 0, "whole consumer warps");
   static_assert(W <= 256, "TMA box extent");
   static_assert(TY % YPT == 0, "rows per thread");
 };
 
-template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
-__global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS)
-    stream3d_kernel(const __grid_constant__ CUtensorMap tmap, const S3Params P) {
+// Arithmetic of one output row: MODE_EXACT follows the reference sum term by
+// term (every product and sum rounded separately); MODE_FAST sums the taps
+// that share a weight first and uses FMA with alpha folded into the weights.
+enum { MODE_EXACT = 0, MODE_FAST = 1 };
+
+struct FastW {
+  float a[3];  // LAP: alpha*w[t] for the off-centre taps t < R (mirror t' = T-1-t); [R]: alpha*D*w[R]
+};              // D1: alpha*w[t] for t > R (antisymmetric: w[T-1-t] = -w[t])
+
+// Work items are (chunk of planes, tile) pairs in chunk-major order, dealt
+// round-robin to a persistent grid: the items in flight at any time share a
+// plane range, so neighbouring tiles read each other's halo rows from L2.
+// The stage ring and its barrier phases continue from one item to the next
+// (running stage counters), so the producer prefetches across items.
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, bool PP0, int MODE>
+__global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS, 2)
+    stream3d_kernel(const __grid_constant__ CUtensorMap tmap, const S3Params P, const FastW FW) {
   using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>;
   constexpr int ROWS = C::ROWS, W = C::W, WP = C::WP, S = C::S, T = 2 * R + 1;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* smem = reinterpret_cast<float*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_FLOATS);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_FLOATS);
+  uint64_t* empty = full + S;
 
-  int bid = blockIdx.x;
-  const int tz = bid % P.nz_tiles;
-  bid /= P.nz_tiles;
-  const int ty = bid % P.ny_tiles;
-  bid /= P.ny_tiles;
-  const int z0 = P.g + tz * TZ, y0 = P.g + ty * TY;
-  const int xs = P.g + bid * P.chunk;
-  const int xe = min(xs + P.chunk, P.X - P.g);
-  if (xs >= xe) return;  // block-uniform
-  const int nout = xe - xs;
-  const int nplanes = nout + 2 * R;
-  const int lane = threadIdx.x, yg = threadIdx.y;
-  const int tid = yg * C::LANES + lane;
-  const int warp = tid >> 5, wl = tid & 31;
-  const int zc = (z0 - R) * CIN;  // float offset of the tile start within a row
+  if ((int)blockIdx.x >= P.nitems) return;  // block-uniform
+  const int nx = P.X - 2 * P.g;
+  const int tid = threadIdx.x;
 
   if (tid == 0) {
-    for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], C::NCW);
+    }
     mbar_fence_init();
   }
   __syncthreads();
 
-  // warp 0 brings plane i (x = xs - R + i) into stage i % S.
-  auto issue = [&](int i) {
-    const int s = i % S;
-    const int x = xs - R + i;
-    if (wl == 0) mbar_arrive_expect_tx(&bar[s], ROWS * W * 4);
-    __syncwarp();
-    if (wl < ROWS) {
-      const int y = y0 - R + wl;
-      const int f0 = (x * P.Y + y) * P.Z * CIN + zc;
-      tma_load_1d(smem + (s * ROWS + wl) * WP, &tmap, f0 & ~3, &bar[s]);
+  if (tid >= C::NCONS) {
+    // ---------------- producer warp ----------------
+    const int wl = tid - C::NCONS;
+    bool dead = false;
+    int s = 0, ph = 0, issued = 0;  // stage, its use parity, planes issued
+    for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+      const int c = item / P.ntiles, tile = item - c * P.ntiles;
+      const int xoff = c * P.chunk, len = min(P.chunk, nx - xoff);
+      const int tz = tile % P.nz_tiles, ty = tile / P.nz_tiles;
+      const int z0 = P.g + tz * TZ, y0 = P.g + ty * TY, xs = P.g + xoff;
+      const int nplanes = len + 2 * R;
+      int rowf = ((xs - R) * P.Y + (y0 - R)) * P.Z * CIN + (z0 - R) * CIN;  // row 0 of plane 0
+      const int plane_f = P.Y * P.Z * CIN, row_f = P.Z * CIN;
+      for (int i = 0; i < nplanes; ++i) {
+        // plane `issued` reuses the stage of plane issued - S: wait for its release
+        if (issued >= S && !dead && !mbar_wait_bounded(&empty[s], (uint32_t)(ph ^ 1))) {
+          dead = true;
+          flag_error(PDE_ERR_TIMEOUT);
+        }
+        if (wl == 0) mbar_arrive_expect_tx(&full[s], ROWS * W * 4);
+        __syncwarp();
+        for (int r = wl; r < ROWS; r += 32)
+          tma_load_1d(smem + (s * ROWS + r) * WP, &tmap, (rowf + r * row_f) & ~3, &full[s]);
+        rowf += plane_f;
+        ++issued;
+        if (++s == S) { s = 0; ph ^= 1; }
+      }
     }
-  };
+    return;
+  }
+
+  // ---------------- consumer threads ----------------
+  const int lane = tid % C::LANES, yg = tid / C::LANES;
+  const bool warp_leader = (tid & 31) == 0;
+  const int cofs = (OP == OP_LAP) ? (R * CIN + lane) : ((R + lane) * CIN);
+  constexpr int qc = 0;                         // x taps: component 0 (DIV: u_x)
+  constexpr int yc = (OP == OP_DIV) ? 1 : 0;    // y taps: DIV reads u_y
+  constexpr int zcmp = (OP == OP_DIV) ? 2 : 0;  // z taps: DIV reads u_z
+  constexpr int zstep = CIN;
+  constexpr int M = YPT + 2 * R;                // centre-plane rows a thread reads
+  const int row0 = yg * YPT;                    // first stage row of the thread's window
+  const float* smem_c = smem + row0 * WP + cofs;
+
+  float w[T];
+#pragma unroll
+  for (int t = 0; t < T; ++t) w[t] = P.w[t];
+  const float alpha = P.alpha;
+
   bool dead = false;
-  auto wait_plane = [&](int i) {
-    if (!dead && !mbar_wait_bounded(&bar[i % S], (uint32_t)((i / S) & 1))) {
+  // consumer stage counters: the newest plane (ns, nph) and the centre plane (cs)
+  int ns = 0, nph = 0, cs = 0;
+  auto adv = [&](int& st) { if (++st == S) st = 0; };
+  auto wait_new = [&]() {
+    if (!dead && !mbar_wait_bounded(&full[ns], (uint32_t)nph)) {
       dead = true;
       flag_error(PDE_ERR_TIMEOUT);
     }
   };
-  // position of the tile's first cell (z0 - R) inside a staged row.
-  auto lead = [&](int x, int y) { return (x * P.pp + y * P.pr + zc) & 3; };
-  auto stage = [&](int i) -> const float* { return smem + (i % S) * C::STAGE_FLOATS; };
+  auto release = [&](int st) {
+    __syncwarp();
+    if (warp_leader) mbar_arrive(&empty[st]);
+  };
 
-  if (warp == 0) {
-    const int pre = nplanes < S ? nplanes : S;
-    for (int i = 0; i < pre; ++i) issue(i);
-  }
+  const int zrow = P.Z * CIN;
+  const int oplane = (OP == OP_LAP) ? P.Y * zrow : P.Y * P.Z * ((OP == OP_GRAD) ? 3 : 1);
+  const int orow = (OP == OP_LAP) ? zrow : P.Z * ((OP == OP_GRAD) ? 3 : 1);
 
-  // Offset (floats) of this thread's centre value inside a staged row,
-  // excluding the row lead.
-  constexpr int zsel = (OP == OP_LAP) ? 0 : 1;
-  const int cofs = (OP == OP_LAP) ? (R * CIN + lane) : ((R + lane) * CIN);
-  // component read from the x-queue / y-column / z-row for each op.
-  constexpr int qc = 0;                         // x taps: component 0 (DIV: u_x)
-  constexpr int yc = (OP == OP_DIV) ? 1 : 0;    // y taps: DIV reads u_y
-  constexpr int zcmp = (OP == OP_DIV) ? 2 : 0;  // z taps: DIV reads u_z
-  constexpr int zstep = (OP == OP_LAP) ? CIN : CIN;
-  (void)zsel;
+  for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+    const int c = item / P.ntiles, tile = item - c * P.ntiles;
+    const int xoff = c * P.chunk, len = min(P.chunk, nx - xoff);
+    const int tz = tile % P.nz_tiles, ty = tile / P.nz_tiles;
+    const int z0 = P.g + tz * TZ, y0 = P.g + ty * TY, xs = P.g + xoff;
+    const int zc = (z0 - R) * CIN;
 
-  float q[T][YPT];
+    // Lead of window row m in plane x: (x*pp + (y0-R+row0+m)*pr + zc) & 3 depends on
+    // m only through m mod 4: off[cl] for class cl = m & 3.
+    const int phi = (y0 - R + row0) & 3;
+    int off[4];
+    auto offsets = [&](int x) {
+      const int l = x * P.pp + zc;
 #pragma unroll
-  for (int t = 0; t < T; ++t)
-#pragma unroll
-    for (int k = 0; k < YPT; ++k) q[t][k] = 0.0f;
+      for (int cl = 0; cl < 4; ++cl) off[cl] = (l + (phi + cl) * P.pr) & 3;
+    };
+    if constexpr (PP0) offsets(0);
 
-  // Pre-load planes 0 .. 2R-1 into q[1 .. 2R].
+    unsigned vmask = 0;
+    const int zcell = (OP == OP_LAP) ? (z0 + lane / CIN) : (z0 + lane);
 #pragma unroll
-  for (int i = 0; i < 2 * R; ++i) {
-    wait_plane(i);
-    const float* sp = stage(i);
-    const int x = xs - R + i;
-#pragma unroll
-    for (int k = 0; k < YPT; ++k) {
-      const int r = R + yg * YPT + k;
-      q[i + 1][k] = sp[r * WP + lead(x, y0 - R + r) + cofs + qc];
-    }
-  }
+    for (int k = 0; k < YPT; ++k)
+      if (y0 + row0 + k < P.Y - P.g && zcell < P.Z - P.g) vmask |= 1u << k;
+    const bool all_rows = vmask == (1u << YPT) - 1u;
+    float* optr = P.out + ((OP == OP_LAP) ? ((xs * P.Y + y0 + row0) * zrow + z0 * CIN + lane)
+                                          : ((xs * P.Y + y0 + row0) * P.Z + zcell) * ((OP == OP_GRAD) ? 3 : 1));
 
-  const float alpha = P.alpha;
-  float w[T];
+    // x-queue: plane p (item-relative) lives in slot p % T
+    float q[T][YPT];
 #pragma unroll
-  for (int t = 0; t < T; ++t) w[t] = P.w[t];
-
-  for (int j = 0; j < nout; ++j) {
-    const int inew = j + 2 * R;
-    wait_plane(inew);
+    for (int i = 0; i < 2 * R; ++i) {
+      wait_new();
+      if constexpr (!PP0) offsets(xs - R + i);
+      const float* sp = smem_c + ns * C::STAGE_FLOATS + qc;
 #pragma unroll
-    for (int t = 0; t < T - 1; ++t)
-#pragma unroll
-      for (int k = 0; k < YPT; ++k) q[t][k] = q[t + 1][k];
-    {
-      const float* sp = stage(inew);
-      const int x = xs - R + inew;
-#pragma unroll
-      for (int k = 0; k < YPT; ++k) {
-        const int r = R + yg * YPT + k;
-        q[T - 1][k] = sp[r * WP + lead(x, y0 - R + r) + cofs + qc];
+      for (int k = 0; k < YPT; ++k) q[i][k] = sp[(R + k) * WP + off[(R + k) & 3]];
+      if (i < R) {  // planes below R are never a centre plane
+        release(cs);
+        adv(cs);
       }
+      adv(ns);
+      if (ns == 0) nph ^= 1;
     }
-    const float* sc = stage(j + R);
-    const int xc = xs + j;
-    float col[YPT + 2 * R];
+
+    for (int j0 = 0; j0 < len; j0 += T) {
+      static_for<0, T>([&](auto JJ) {
+        constexpr int jj = decltype(JJ)::value;
+        const int j = j0 + jj;
+        if (j >= len) return;
+        wait_new();
+        if constexpr (!PP0) offsets(xs + R + j);
+        {
+          const float* sp = smem_c + ns * C::STAGE_FLOATS + qc;
 #pragma unroll
-    for (int m = 0; m < YPT + 2 * R; ++m) {
-      const int r = yg * YPT + m;
-      col[m] = sc[r * WP + lead(xc, y0 - R + r) + cofs + yc];
-    }
+          for (int k = 0; k < YPT; ++k) q[(jj + 2 * R) % T][k] = sp[(R + k) * WP + off[(R + k) & 3]];
+        }
+        adv(ns);
+        if (ns == 0) nph ^= 1;
+        if constexpr (!PP0) offsets(xs + j);
+        const float* sc = smem_c + cs * C::STAGE_FLOATS;
+        float col[M];
 #pragma unroll
-    for (int k = 0; k < YPT; ++k) {
-      const int r = R + yg * YPT + k;
-      const int yk = y0 - R + r;
-      const float* rowp = sc + r * WP + lead(xc, yk) + cofs + zcmp;
-      if constexpr (OP == OP_LAP || OP == OP_DIV) {
-        float acc = 0.0f;
+        for (int m = 0; m < M; ++m) col[m] = sc[m * WP + off[m & 3] + yc];
+        float res[YPT][(OP == OP_GRAD) ? 3 : 1];
 #pragma unroll
-        for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], q[t][k]));
+        for (int k = 0; k < YPT; ++k) {
+          const float* rowp = sc + (R + k) * WP + off[(R + k) & 3] + zcmp;
+          auto xq = [&](int t) { return q[(jj + t) % T][k]; };
+          auto zt = [&](int t) { return (t == R && OP == OP_LAP) ? col[k + R] : rowp[(t - R) * zstep]; };
+          if constexpr (MODE == MODE_EXACT) {
+            if constexpr (OP == OP_LAP || OP == OP_DIV) {
+              float acc = mul(w[0], xq(0));
 #pragma unroll
-        for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], col[k + t]));
+              for (int t = 1; t < T; ++t) acc = add(acc, mul(w[t], xq(t)));
 #pragma unroll
-        for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], rowp[(t - R) * zstep]));
-        const float res = mul(alpha, acc);
-        if (OP == OP_LAP) {
-          const int zcell = z0 + lane / CIN;
-          if (yk < P.Y - P.g && zcell < P.Z - P.g)
-            P.out[(xc * P.Y + yk) * P.Z * CIN + z0 * CIN + lane] = res;
+              for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], col[k + t]));
+#pragma unroll
+              for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], zt(t)));
+              res[k][0] = mul(alpha, acc);
+            } else {
+              float ax = mul(w[0], xq(0));
+#pragma unroll
+              for (int t = 1; t < T; ++t) ax = add(ax, mul(w[t], xq(t)));
+              float ay = mul(w[0], col[k]);
+#pragma unroll
+              for (int t = 1; t < T; ++t) ay = add(ay, mul(w[t], col[k + t]));
+              float az = mul(w[0], rowp[-R * zstep]);
+#pragma unroll
+              for (int t = 1; t < T; ++t) az = add(az, mul(w[t], t == R ? col[k + R] : rowp[(t - R) * zstep]));
+              res[k][0] = mul(alpha, ax);
+              res[k][1] = mul(alpha, ay);
+              res[k][2] = mul(alpha, az);
+            }
+          } else {
+            if constexpr (OP == OP_LAP) {
+              // alpha*(sum_t w[t]*(x,y,z taps)) = a[R]*centre + sum_{t<R} a[t]*(six mirrored taps)
+              float acc = FW.a[R] * col[k + R];
+#pragma unroll
+              for (int t = 0; t < R; ++t) {
+                const float s6 = ((xq(t) + xq(T - 1 - t)) + (col[k + t] + col[k + T - 1 - t])) +
+                                 (zt(t) + zt(T - 1 - t));
+                acc = fmaf(FW.a[t], s6, acc);
+              }
+              res[k][0] = acc;
+            } else if constexpr (OP == OP_DIV) {
+              // alpha*sum_a sum_{t>R} w[t]*(u_a[+] - u_a[-])
+              float acc = 0.0f;
+#pragma unroll
+              for (int t = R + 1; t < T; ++t) {
+                const float d3 = ((xq(t) - xq(T - 1 - t)) + (col[k + t] - col[k + T - 1 - t])) +
+                                 (zt(t) - zt(T - 1 - t));
+                acc = (t == R + 1) ? FW.a[t - R - 1] * d3 : fmaf(FW.a[t - R - 1], d3, acc);
+              }
+              res[k][0] = acc;
+            } else {
+              float ax = 0.0f, ay = 0.0f, az = 0.0f;
+#pragma unroll
+              for (int t = R + 1; t < T; ++t) {
+                const float a = FW.a[t - R - 1];
+                const bool first = (t == R + 1);
+                ax = first ? a * (xq(t) - xq(T - 1 - t)) : fmaf(a, xq(t) - xq(T - 1 - t), ax);
+                ay = first ? a * (col[k + t] - col[k + T - 1 - t]) : fmaf(a, col[k + t] - col[k + T - 1 - t], ay);
+                az = first ? a * (rowp[(t - R) * zstep] - rowp[(R - t) * zstep])
+                           : fmaf(a, rowp[(t - R) * zstep] - rowp[(R - t) * zstep], az);
+              }
+              res[k][0] = ax;
+              res[k][1] = ay;
+              res[k][2] = az;
+            }
+          }
+        }
+        release(cs);  // the centre plane is not read again
+        adv(cs);
+        float* op = optr + j * oplane;
+        if (all_rows) {
+#pragma unroll
+          for (int k = 0; k < YPT; ++k) {
+            if constexpr (OP == OP_GRAD) {
+              op[k * orow + 0] = res[k][0];
+              op[k * orow + 1] = res[k][1];
+              op[k * orow + 2] = res[k][2];
+            } else {
+              op[k * orow] = res[k][0];
+            }
+          }
         } else {
-          const int zcell = z0 + lane;
-          if (yk < P.Y - P.g && zcell < P.Z - P.g) P.out[(xc * P.Y + yk) * P.Z + zcell] = res;
+#pragma unroll
+          for (int k = 0; k < YPT; ++k) {
+            if (!((vmask >> k) & 1u)) continue;
+            if constexpr (OP == OP_GRAD) {
+              op[k * orow + 0] = res[k][0];
+              op[k * orow + 1] = res[k][1];
+              op[k * orow + 2] = res[k][2];
+            } else {
+              op[k * orow] = res[k][0];
+            }
+          }
         }
-      } else {  // OP_GRAD: scalar in, (d/dx, d/dy, d/dz) out
-        float ax = 0.0f, ay = 0.0f, az = 0.0f;
-#pragma unroll
-        for (int t = 0; t < T; ++t) ax = add(ax, mul(w[t], q[t][k]));
-#pragma unroll
-        for (int t = 0; t < T; ++t) ay = add(ay, mul(w[t], col[k + t]));
-#pragma unroll
-        for (int t = 0; t < T; ++t) az = add(az, mul(w[t], rowp[(t - R) * zstep]));
-        const int zcell = z0 + lane;
-        if (yk < P.Y - P.g && zcell < P.Z - P.g) {
-          float* o = P.out + ((size_t)((xc * P.Y + yk) * P.Z + zcell)) * 3;
-          o[0] = mul(alpha, ax);
-          o[1] = mul(alpha, ay);
-          o[2] = mul(alpha, az);
-        }
-      }
+      });
     }
-    __syncthreads();  // every thread is done with plane j's stage
-    if (warp == 0 && j + S < nplanes) issue(j + S);
+    // the last R planes were read only into the x-queue
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      release(cs);
+      adv(cs);
+    }
   }
 }
 
