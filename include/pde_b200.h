@@ -212,6 +212,22 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
                      int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
                      int32_t nsteps, int32_t steps_per_pass, void* stream);
 
+/* Allocation-free variant of pde_heat_rollout.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory (a memory manager
+ * owns every allocation, cudaMalloc is not allowed in a latency-critical loop,
+ * or a foreign-language host can only pass the field buffers it holds): the
+ * scratch field comes from a fixed device array inside this library, of
+ * PDE_NOALLOC_MAX_FLOATS floats (16 MiB), held on every GPU that loads the
+ * library until the process exits.  Grids with X*Y*Z*ncomp above that return
+ * PDE_ERR_TOO_LARGE.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race, so serialise them.
+ * Arguments and results are those of pde_heat_rollout without `work`. */
+#define PDE_NOALLOC_MAX_FLOATS (1 << 22)
+int pde_heat_rollout_noalloc(const float* u_in, float* u_out, const PdeGrid* grid, int32_t ncomp,
+                             const PdeBCRules* rules, float alpha, float dt, int32_t nsteps,
+                             int32_t steps_per_pass, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,7 @@ PDE_BC_FUNC_CONSTANT = 0
 PDE_BC_FUNC_RAMP = 1
 PDE_FUSED_MAX_COMP = 4
 PDE_MAX_GROUPS = 16
+PDE_NOALLOC_MAX_FLOATS = 1 << 22
 FACE_BITS = {"-X": 1 << 0, "+X": 1 << 1, "-Y": 1 << 2, "+Y": 1 << 3, "-Z": 1 << 4, "+Z": 1 << 5}
 
 
@@ -96,6 +97,9 @@ _SIGS = {
     "pde_heat_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                    C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                    C.c_void_p]),
+    "pde_heat_rollout_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
+                                           C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
+                                           C.c_void_p]),
 }
 
 _lib = None
