@@ -24,9 +24,10 @@ are restated from their definitions.  Pass ``dtype=np.float64`` for the
 float64 oracle (same operation order, double rounding).
 
 Parity pin: the reference package imports ``warp`` (warp-lang 1.12.1, not
-installed here), so its kernels are executed through the Warp-DSL emulator in
-oracle/warp_emu.py by tests/golden/make_golden.py; the fixtures it writes pin
-this restatement (tests/test_oracle_golden.py).
+installed here), so tests/golden/make_golden.py runs the reference's own FDM
+modules through the Warp-DSL executor tests/golden/warp_emu.py and stores their
+outputs in tests/golden/fdm_golden.npz; tests/test_golden_cpu.py checks this
+restatement against them bit for bit.
 """
 from __future__ import annotations
 
