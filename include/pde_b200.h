@@ -127,6 +127,17 @@ int         pde_device_error(void* stream);
 #define PDE_DISPATCH_GENERIC 1
 int         pde_set_dispatch(int mode);
 
+/* Tile configuration of the 3D streaming kernel used for one operator and
+ * order: candidate 0 (default) .. 3; op is PDE_OP_*, ncomp_in the input's
+ * component count (Laplacian 1 or 3, Grad 1, Divergence 3).  Candidates above
+ * 0 apply to exact mode on grids with even Y and Z (others keep candidate 0).  candidate -1 queries.  Process-wide; returns the
+ * previous candidate or a negative status.  The tuner in
+ * pde_module_b200/tuning.py sweeps these. */
+#define PDE_OP_LAPLACIAN  0
+#define PDE_OP_GRAD       1
+#define PDE_OP_DIVERGENCE 2
+int         pde_stream3d_select(int32_t op, int32_t order, int32_t ncomp_in, int32_t candidate);
+
 /* ---- operators (one launch each; out must not alias in) ------------- */
 
 /* out[c] = alpha * sum_{axis} sum_{tap} w[tap] * in[c + shift*e_axis], per component,

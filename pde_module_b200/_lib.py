@@ -29,6 +29,9 @@ PDE_MODE_EXACT = 0
 PDE_MODE_FAST = 1
 PDE_DISPATCH_AUTO = 0
 PDE_DISPATCH_GENERIC = 1
+PDE_OP_LAPLACIAN = 0
+PDE_OP_GRAD = 1
+PDE_OP_DIVERGENCE = 2
 PDE_BC_DIRICHLET = 1
 PDE_BC_VON_NEUMANN = 2
 PDE_BC_FUNC_CONSTANT = 0
@@ -79,6 +82,7 @@ _SIGS = {
     "pde_strerror": (C.c_char_p, [C.c_int]),
     "pde_device_error": (C.c_int, [C.c_void_p]),
     "pde_set_dispatch": (C.c_int, [C.c_int]),
+    "pde_stream3d_select": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
     "pde_laplacian": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_void_p]),
     "pde_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_void_p]),
     "pde_divergence": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_float, C.c_void_p]),

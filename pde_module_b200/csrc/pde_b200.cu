@@ -31,11 +31,11 @@ int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ER
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // ---- 3D streaming dispatch -------------------------------------------------
-template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, bool PP0, int MODE>
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK, int MODE>
 int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& Wt, double alpha_d, float alpha,
                       cudaStream_t st) {
-  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>;
-  auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF, PP0, MODE>;
+  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>;
+  auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>;
   static int occ = -1;
   if (occ < 0) {
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM) != cudaSuccess)
@@ -80,7 +80,14 @@ int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& 
   P.nitems = P.ntiles * nchunks;
   long long blocks = slots < P.nitems ? slots : P.nitems;
   CUtensorMap m;
-  if (!encode_1d(&m, in, (uint64_t)total, (uint32_t)C::W)) return PDE_ERR_CUDA;
+  if (MAPK == MAP_PAIRS) {
+    const uint64_t zc = (uint64_t)G.n[2] * CIN;
+    if (!encode_3d(&m, in, 2 * zc, (uint64_t)G.n[1] / 2, (uint64_t)G.n[0], 8 * zc, 4 * zc * (uint64_t)G.n[1],
+                   (uint32_t)C::W, (uint32_t)(C::ROWS / 2)))
+      return PDE_ERR_CUDA;
+  } else if (!encode_1d(&m, in, (uint64_t)total, (uint32_t)C::W)) {
+    return PDE_ERR_CUDA;
+  }
   FastW FW{};
   if (MODE == MODE_FAST) {
     // folded weights from the double-precision stencil (Weights::wd)
@@ -95,16 +102,84 @@ int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& 
   return launch_status();
 }
 
+// Plane addressing for a grid: double-row boxes when the array's row pairs and
+// planes have 16-byte multiple pitches and the tile rows start on even rows;
+// else one copy per row (lead fixed across planes when the plane pitch is a
+// multiple of 4 floats).
+template <int CIN>
+int pick_map(const Geo& G, int R) {
+  const int64_t zc = G.n[2] * CIN;
+  if ((G.n[1] % 2) == 0 && (zc % 2) == 0 && ((G.n[1] * zc) % 4) == 0 && ((G.g - R) % 2) == 0 &&
+      G.n[1] / 2 < (1LL << 31) && 2 * zc < (1LL << 31))
+    return MAP_PAIRS;
+  return ((G.n[1] * zc) & 3) == 0 ? MAP_ROWS_PP0 : MAP_ROWS_GEN;
+}
+
 template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
 int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt, float alpha, int mode,
                     cudaStream_t st) {
-  const bool pp0 = ((G.n[1] * G.n[2] * CIN) & 3) == 0;
+  const int map = pick_map<CIN>(G, R);
   if (mode == PDE_MODE_FAST) {
-    if (pp0) return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, true, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
-    return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, false, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
+    if (map == MAP_PAIRS)
+      return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, MAP_PAIRS, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
+    if (map == MAP_ROWS_PP0)
+      return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, MAP_ROWS_PP0, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
+    return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, MAP_ROWS_GEN, MODE_FAST>(in, out, G, Wt, alpha, alpha, st);
   }
-  if (pp0) return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, true, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
-  return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, false, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
+  if (map == MAP_PAIRS)
+    return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, MAP_PAIRS, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
+  if (map == MAP_ROWS_PP0)
+    return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, MAP_ROWS_PP0, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
+  return launch_stream3d_k<R, OP, CIN, TZ, TY, YPT, PREF, MAP_ROWS_GEN, MODE_EXACT>(in, out, G, Wt, alpha, alpha, st);
+}
+
+// Tile configurations of the streaming kernels.  Candidate 0 is the default
+// for every shape and mode; candidates 1-3 are compiled for double-row
+// addressing (even Y and Z), exact arithmetic, and are picked per
+// (operator, order) by pde_stream3d_select (the autotuner sweeps them).
+enum { S3K_LAP1 = 0, S3K_LAP3 = 1, S3K_GRAD = 2, S3K_DIV = 3, S3K_KINDS = 4 };
+// Defaults [kind][order 2, order 4]: the fastest candidates of a sweep at 512^3 on B200.
+int g_s3_sel[S3K_KINDS][2] = {{2, 2}, {3, 3}, {1, 1}, {1, 1}};
+constexpr int kS3Candidates = 4;
+
+template <int R, int OP, int CIN>
+int launch_candidate(int cand, const float* in, float* out, const Geo& G, const Weights& W, float alpha,
+                     cudaStream_t st) {
+  if constexpr (OP == OP_LAP && CIN == 1) {
+    switch (cand) {
+      case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 1, 64, 32, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+    }
+  } else if constexpr (OP == OP_LAP) {
+    switch (cand) {
+      case 1: return launch_stream3d_k<R, OP, 3, 32, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 2: return launch_stream3d_k<R, OP, 3, 64, 8, 8, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 3, 32, 32, 8, 2, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+    }
+  } else if constexpr (OP == OP_GRAD) {
+    switch (cand) {
+      case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 1, 64, 32, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+    }
+  } else {
+    switch (cand) {
+      case 1: return launch_stream3d_k<R, OP, 3, 64, 16, 4, 2, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 2: return launch_stream3d_k<R, OP, 3, 32, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 3, 64, 32, 8, 1, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+    }
+  }
+}
+
+// Launch the selected candidate when it applies, else the default configuration.
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
+int launch_selected(int kind, const float* in, float* out, const Geo& G, const Weights& W, float alpha, int mode,
+                    cudaStream_t st) {
+  const int cand = g_s3_sel[kind][R - 1];
+  if (cand > 0 && mode == PDE_MODE_EXACT && pick_map<CIN>(G, R) == MAP_PAIRS)
+    return launch_candidate<R, OP, CIN>(cand, in, out, G, W, alpha, st);
+  return launch_stream3d<R, OP, CIN, TZ, TY, YPT, PREF>(in, out, G, W, alpha, mode, st);
 }
 
 // The flat 1D TMA view addresses floats with int32 coordinates, including rows
@@ -134,6 +209,21 @@ int check_common(const void* in, const void* out, const PdeGrid* grid, int ncomp
 extern "C" {
 
 int pde_version(void) { return 100; }
+
+int pde_stream3d_select(int32_t op, int32_t order, int32_t ncomp_in, int32_t candidate) {
+  int kind;
+  if (op == PDE_OP_LAPLACIAN && ncomp_in == 1) kind = S3K_LAP1;
+  else if (op == PDE_OP_LAPLACIAN && ncomp_in == 3) kind = S3K_LAP3;
+  else if (op == PDE_OP_GRAD && ncomp_in == 1) kind = S3K_GRAD;
+  else if (op == PDE_OP_DIVERGENCE && ncomp_in == 3) kind = S3K_DIV;
+  else return PDE_ERR_UNSUPPORTED;
+  if (order != 2 && order != 4) return PDE_ERR_ARG;
+  if (candidate < -1 || candidate >= kS3Candidates) return PDE_ERR_ARG;
+  int& slot = g_s3_sel[kind][order / 2 - 1];
+  const int prev = slot;
+  if (candidate >= 0) slot = candidate;
+  return prev;
+}
 
 int pde_set_dispatch(int mode) {
   const int prev = g_dispatch;
@@ -178,11 +268,11 @@ int pde_laplacian_ex(const float* in, float* out, const PdeGrid* grid, int32_t n
   cudaStream_t st = as_stream(stream);
   if ((ncomp == 1 || ncomp == 3) && stream3d_ok(in, G, ncomp)) {
     if (G.order == 2) {
-      if (ncomp == 1) return launch_stream3d<1, OP_LAP, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
-      return launch_stream3d<1, OP_LAP, 3, 32, 16, 8, 4>(in, out, G, W, alpha, mode, st);
+      if (ncomp == 1) return launch_selected<1, OP_LAP, 1, 64, 32, 8, 4>(S3K_LAP1, in, out, G, W, alpha, mode, st);
+      return launch_selected<1, OP_LAP, 3, 32, 16, 8, 4>(S3K_LAP3, in, out, G, W, alpha, mode, st);
     } else {
-      if (ncomp == 1) return launch_stream3d<2, OP_LAP, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
-      return launch_stream3d<2, OP_LAP, 3, 32, 16, 8, 4>(in, out, G, W, alpha, mode, st);
+      if (ncomp == 1) return launch_selected<2, OP_LAP, 1, 64, 32, 8, 4>(S3K_LAP1, in, out, G, W, alpha, mode, st);
+      return launch_selected<2, OP_LAP, 3, 32, 16, 8, 4>(S3K_LAP3, in, out, G, W, alpha, mode, st);
     }
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp;
@@ -205,8 +295,8 @@ int pde_grad_ex(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
   const Weights W = d1_weights(G.order, grid->dx);
   cudaStream_t st = as_stream(stream);
   if (ncomp == 1 && stream3d_ok(in, G, 1)) {
-    if (G.order == 2) return launch_stream3d<1, OP_GRAD, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
-    return launch_stream3d<2, OP_GRAD, 1, 64, 32, 8, 4>(in, out, G, W, alpha, mode, st);
+    if (G.order == 2) return launch_selected<1, OP_GRAD, 1, 64, 32, 8, 4>(S3K_GRAD, in, out, G, W, alpha, mode, st);
+    return launch_selected<2, OP_GRAD, 1, 64, 32, 8, 4>(S3K_GRAD, in, out, G, W, alpha, mode, st);
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp * G.ndims;
   const int blocks = grid_blocks(total, 256);
@@ -228,8 +318,8 @@ int pde_divergence_ex(const float* in, float* out, const PdeGrid* grid, int32_t 
   const Weights W = d1_weights(G.order, grid->dx);
   cudaStream_t st = as_stream(stream);
   if (nrows == 1 && stream3d_ok(in, G, 3)) {
-    if (G.order == 2) return launch_stream3d<1, OP_DIV, 3, 64, 16, 8, 2>(in, out, G, W, alpha, mode, st);
-    return launch_stream3d<2, OP_DIV, 3, 64, 16, 8, 2>(in, out, G, W, alpha, mode, st);
+    if (G.order == 2) return launch_selected<1, OP_DIV, 3, 64, 16, 8, 2>(S3K_DIV, in, out, G, W, alpha, mode, st);
+    return launch_selected<2, OP_DIV, 3, 64, 16, 8, 2>(S3K_DIV, in, out, G, W, alpha, mode, st);
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * nrows;
   const int blocks = grid_blocks(total, 256);

@@ -47,7 +47,15 @@ __device__ __forceinline__ void static_for(F&& f) {
   }
 }
 
-template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF>
+// Plane addressing: MAP_ROWS_GEN / MAP_ROWS_PP0 bring each tile row with its
+// own 1D TMA copy (the lead of a row inside its 16-byte aligned copy varies
+// with the plane in the GEN case, is fixed in the PP0 case); MAP_PAIRS views
+// the array as (2*Z*CIN, Y/2, X) "double rows" (pitch 8*Z*CIN bytes, a
+// multiple of 16 when Z is even), so a plane tile arrives as two 2D boxes:
+// the even rows and the odd rows.
+enum { MAP_ROWS_GEN = 0, MAP_ROWS_PP0 = 1, MAP_PAIRS = 2 };
+
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK = MAP_ROWS_PP0>
 struct S3Cfg {
   static constexpr int LANES = (OP == OP_LAP) ? TZ * CIN : TZ;  // consumer threads per row group
   static constexpr int TYG = TY / YPT;                           // row groups
@@ -58,9 +66,13 @@ struct S3Cfg {
   static constexpr int W = round4(3 + (TZ + 2 * R) * CIN);  // TMA box (floats)
   static constexpr int WP = (W + 31) & ~31;                 // smem row pitch: 128-byte aligned rows
   static constexpr int S = R + 1 + PREF;                    // stages: centre .. newest + prefetch
-  static constexpr int STAGE_FLOATS = ROWS * WP;
+  // MAP_PAIRS: each half (even / odd rows) is a dense [ROWS/2][W] box, 128-byte aligned
+  static constexpr int HALF = ((ROWS / 2) * W + 31) & ~31;
+  static constexpr int STAGE_FLOATS = (MAPK == MAP_PAIRS) ? 2 * HALF : ROWS * WP;
+  // Grad: per consumer warp, YPT rows x 32 cells x 3 outputs staged for contiguous stores
+  static constexpr int OBUF_FLOATS = (OP == OP_GRAD) ? NCW * YPT * 96 : 0;
   // + 128: the base is rounded up to a 128-byte boundary at run time
-  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)2 * S * 8 + 128;
+  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)2 * S * 8 + (size_t)OBUF_FLOATS * 4 + 128;
   static_assert(NCONS % 32 == 0, "whole consumer warps");
   static_assert(W <= 256, "TMA box extent");
   static_assert(TY % YPT == 0, "rows per thread");
@@ -80,15 +92,17 @@ struct FastW {
 // plane range, so neighbouring tiles read each other's halo rows from L2.
 // The stage ring and its barrier phases continue from one item to the next
 // (running stage counters), so the producer prefetches across items.
-template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, bool PP0, int MODE>
-__global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS, 2)
+template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK, int MODE>
+__global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::THREADS, 2)
     stream3d_kernel(const __grid_constant__ CUtensorMap tmap, const S3Params P, const FastW FW) {
-  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>;
+  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>;
+  constexpr bool PP0 = (MAPK != MAP_ROWS_GEN);
   constexpr int ROWS = C::ROWS, W = C::W, WP = C::WP, S = C::S, T = 2 * R + 1;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* smem = reinterpret_cast<float*>(smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * C::STAGE_FLOATS);
   uint64_t* empty = full + S;
+  float* obuf = reinterpret_cast<float*>(empty + S);
 
   if ((int)blockIdx.x >= P.nitems) return;  // block-uniform
   const int nx = P.X - 2 * P.g;
@@ -124,8 +138,15 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
         }
         if (wl == 0) mbar_arrive_expect_tx(&full[s], ROWS * W * 4);
         __syncwarp();
-        for (int r = wl; r < ROWS; r += 32)
-          tma_load_1d(smem + (s * ROWS + r) * WP, &tmap, (rowf + r * row_f) & ~3, &full[s]);
+        if constexpr (MAPK == MAP_PAIRS) {
+          // even rows (p = 0) and odd rows (p = 1) of the tile: (y0 - R) is even
+          if (wl < 2)
+            tma_load_3d(smem + s * C::STAGE_FLOATS + wl * C::HALF, &tmap, (wl * row_f + (z0 - R) * CIN) & ~3,
+                        (y0 - R) >> 1, xs - R + i, &full[s]);
+        } else {
+          for (int r = wl; r < ROWS; r += 32)
+            tma_load_1d(smem + (s * ROWS + r) * WP, &tmap, (rowf + r * row_f) & ~3, &full[s]);
+        }
         rowf += plane_f;
         ++issued;
         if (++s == S) { s = 0; ph ^= 1; }
@@ -144,7 +165,14 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
   constexpr int zstep = CIN;
   constexpr int M = YPT + 2 * R;                // centre-plane rows a thread reads
   const int row0 = yg * YPT;                    // first stage row of the thread's window
-  const float* smem_c = smem + row0 * WP + cofs;
+  // offset (floats) of window row m (stage row row0 + m) inside a stage, without its lead;
+  // MAP_PAIRS: row0 is even (YPT even), so row0 + m has the parity of m
+  static_assert(MAPK != MAP_PAIRS || (YPT % 2 == 0), "pairs need an even row count per thread");
+  auto rowoff = [&](int m) -> int {
+    if constexpr (MAPK == MAP_PAIRS) return (m & 1) * C::HALF + (m >> 1) * W;
+    else return m * WP;
+  };
+  const float* smem_c = smem + ((MAPK == MAP_PAIRS) ? (row0 >> 1) * W : row0 * WP) + cofs;
 
   float w[T];
 #pragma unroll
@@ -178,13 +206,19 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
     const int zc = (z0 - R) * CIN;
 
     // Lead of window row m in plane x: (x*pp + (y0-R+row0+m)*pr + zc) & 3 depends on
-    // m only through m mod 4: off[cl] for class cl = m & 3.
+    // m only through m mod 4: off[cl] for class cl = m & 3.  MAP_PAIRS: the lead
+    // of a row depends only on its parity (off[0], off[1]).
     const int phi = (y0 - R + row0) & 3;
     int off[4];
     auto offsets = [&](int x) {
-      const int l = x * P.pp + zc;
+      if constexpr (MAPK == MAP_PAIRS) {
 #pragma unroll
-      for (int cl = 0; cl < 4; ++cl) off[cl] = (l + (phi + cl) * P.pr) & 3;
+        for (int cl = 0; cl < 4; ++cl) off[cl] = ((cl & 1) * P.Z * CIN + zc) & 3;
+      } else {
+        const int l = x * P.pp + zc;
+#pragma unroll
+        for (int cl = 0; cl < 4; ++cl) off[cl] = (l + (phi + cl) * P.pr) & 3;
+      }
     };
     if constexpr (PP0) offsets(0);
 
@@ -205,7 +239,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
       if constexpr (!PP0) offsets(xs - R + i);
       const float* sp = smem_c + ns * C::STAGE_FLOATS + qc;
 #pragma unroll
-      for (int k = 0; k < YPT; ++k) q[i][k] = sp[(R + k) * WP + off[(R + k) & 3]];
+      for (int k = 0; k < YPT; ++k) q[i][k] = sp[rowoff(R + k) + off[(R + k) & 3]];
       if (i < R) {  // planes below R are never a centre plane
         release(cs);
         adv(cs);
@@ -224,7 +258,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
         {
           const float* sp = smem_c + ns * C::STAGE_FLOATS + qc;
 #pragma unroll
-          for (int k = 0; k < YPT; ++k) q[(jj + 2 * R) % T][k] = sp[(R + k) * WP + off[(R + k) & 3]];
+          for (int k = 0; k < YPT; ++k) q[(jj + 2 * R) % T][k] = sp[rowoff(R + k) + off[(R + k) & 3]];
         }
         adv(ns);
         if (ns == 0) nph ^= 1;
@@ -232,11 +266,11 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
         const float* sc = smem_c + cs * C::STAGE_FLOATS;
         float col[M];
 #pragma unroll
-        for (int m = 0; m < M; ++m) col[m] = sc[m * WP + off[m & 3] + yc];
+        for (int m = 0; m < M; ++m) col[m] = sc[rowoff(m) + off[m & 3] + yc];
         float res[YPT][(OP == OP_GRAD) ? 3 : 1];
 #pragma unroll
         for (int k = 0; k < YPT; ++k) {
-          const float* rowp = sc + (R + k) * WP + off[(R + k) & 3] + zcmp;
+          const float* rowp = sc + rowoff(R + k) + off[(R + k) & 3] + zcmp;
           auto xq = [&](int t) { return q[(jj + t) % T][k]; };
           auto zt = [&](int t) { return (t == R && OP == OP_LAP) ? col[k + R] : rowp[(t - R) * zstep]; };
           if constexpr (MODE == MODE_EXACT) {
@@ -304,28 +338,39 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF>::THREADS,
         release(cs);  // the centre plane is not read again
         adv(cs);
         float* op = optr + j * oplane;
-        if (all_rows) {
+        if constexpr (OP == OP_GRAD) {
+          // The warp's 32 cells of a row own 96 consecutive output floats: stage them
+          // in shared memory and store them as 3 coalesced 128-byte rows.
+          const int wl = tid & 31;
+          float* wb = obuf + (tid >> 5) * (YPT * 96);
 #pragma unroll
           for (int k = 0; k < YPT; ++k) {
-            if constexpr (OP == OP_GRAD) {
-              op[k * orow + 0] = res[k][0];
-              op[k * orow + 1] = res[k][1];
-              op[k * orow + 2] = res[k][2];
-            } else {
-              op[k * orow] = res[k][0];
+            wb[k * 96 + wl * 3 + 0] = res[k][0];
+            wb[k * 96 + wl * 3 + 1] = res[k][1];
+            wb[k * 96 + wl * 3 + 2] = res[k][2];
+          }
+          __syncwarp();
+          // op points at this lane's cell (3 floats); the warp's span starts 3*wl floats earlier
+          float* ob = op - 3 * wl;
+          const int zspan = zcell - wl;  // first cell of the warp's span
+#pragma unroll
+          for (int k = 0; k < YPT; ++k) {
+            const bool rowok = (y0 + row0 + k) < P.Y - P.g;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+              const int f = wl + 32 * i;
+              if (rowok && zspan + f / 3 < P.Z - P.g) ob[k * orow + f] = wb[k * 96 + f];
             }
           }
+          __syncwarp();
+        } else if (all_rows) {
+#pragma unroll
+          for (int k = 0; k < YPT; ++k) op[k * orow] = res[k][0];
         } else {
 #pragma unroll
           for (int k = 0; k < YPT; ++k) {
             if (!((vmask >> k) & 1u)) continue;
-            if constexpr (OP == OP_GRAD) {
-              op[k * orow + 0] = res[k][0];
-              op[k * orow + 1] = res[k][1];
-              op[k * orow + 2] = res[k][2];
-            } else {
-              op[k * orow] = res[k][0];
-            }
+            op[k * orow] = res[k][0];
           }
         }
       });

@@ -163,33 +163,41 @@ def _sample_cells(shape, g, m, rng):
 
 
 @pytest.mark.parametrize("order", [2, 4])
-def test_streaming_vs_generic_and_samples_large(order, rng):
-    """Full-size-class check: the TMA streaming kernels agree bitwise with the
-    general kernels over a 260^3-class grid, and with the oracle at sampled cells."""
+@pytest.mark.parametrize("yz", [(203, 262), (202, 264)])
+@pytest.mark.parametrize("cand", [0, 1, 2, 3])
+def test_streaming_vs_generic_and_samples_large(order, yz, cand, rng):
+    """Full-size-class check: the TMA streaming kernels (per-row copies for odd Y,
+    double-row boxes for even Y and Z; every tile candidate) agree bitwise with
+    the general kernels over a ~200x200x260 grid, and with the oracle at sampled cells."""
     g = order // 2
-    shape = (200, 203, 262 + 2 * g)
+    shape = (200, yz[0], yz[1] + 2 * g)
     dx = 1.0 / 512
     L = _lib.lib()
     u = torch.randn(shape + (1,), device="cuda")
     v = torch.randn(shape + (3,), device="cuda")
+    sel = [(_lib.PDE_OP_LAPLACIAN, 1), (_lib.PDE_OP_LAPLACIAN, 3), (_lib.PDE_OP_GRAD, 1), (_lib.PDE_OP_DIVERGENCE, 3)]
     outs = {}
-    for mode in (_lib.PDE_DISPATCH_GENERIC if hasattr(_lib, "PDE_DISPATCH_GENERIC") else 1, 0):
+    for mode in (_lib.PDE_DISPATCH_GENERIC, _lib.PDE_DISPATCH_AUTO):
         L.pde_set_dispatch(mode)
+        for op, cin in sel:
+            L.pde_stream3d_select(op, order, cin, cand)
         try:
             lap = P.Laplacian(1, dx, g, order=order)(u, 1.0).clone()
             grd = P.Grad(1, shape, dx, g, order=order)(u, 1.0).clone()
             div = P.Divergence(3, shape, dx, g, order=order)(v, 1.0).clone()
             lap3 = P.Laplacian(3, dx, g, order=order)(v, 0.5).clone()
         finally:
-            L.pde_set_dispatch(0)
+            L.pde_set_dispatch(_lib.PDE_DISPATCH_AUTO)
+            for op, cin in sel:
+                L.pde_stream3d_select(op, order, cin, 0)
         outs[mode] = (lap, grd, div, lap3)
-    for a, b in zip(outs[1], outs[0]):
+    for a, b in zip(outs[_lib.PDE_DISPATCH_GENERIC], outs[_lib.PDE_DISPATCH_AUTO]):
         assert torch.equal(a, b)
     assert _lib.device_error() == 0
     un, vn = u.cpu().numpy(), v.cpu().numpy()
     cells = _sample_cells(shape, g, 2000, rng)
     lw, dw = fdm.lap_weights(order, dx), fdm.d1_weights(order, dx)
-    lap, grd, div, lap3 = (t.cpu().numpy() for t in outs[0])
+    lap, grd, div, lap3 = (t.cpu().numpy() for t in outs[_lib.PDE_DISPATCH_AUTO])
     ref = fdm.stencil_at(un, cells, lw, [(0, 0), (1, 0), (2, 0)], 1.0)
     assert np.array_equal(lap[cells[:, 0], cells[:, 1], cells[:, 2], 0], ref)
     for a in range(3):
