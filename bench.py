@@ -223,8 +223,8 @@ def run_ours(args):
 
     # autotune the streaming kernels' tile configuration for this shape (setup, untimed)
     from pde_module_b200 import tuning
-    tuned = tuning.tune_stream3d((N_INT, N_INT, N_INT), reps=3,
-                                 kinds=[("laplacian", 1), ("grad", 1), ("divergence", 3)])
+    tuned = {} if args.no_tune else tuning.tune_stream3d(
+        (N_INT, N_INT, N_INT), reps=3, kinds=[("laplacian", 1), ("grad", 1), ("divergence", 3)])
 
     ops = []
     for order in (2, 4):
@@ -497,6 +497,41 @@ def run_e2e(fields, ops, world, args):
             "path": "pinned host fields -> H2D -> module calls (C ABI) -> D2H of every output"}
 
 
+def run_profile_op(args):
+    """One operator on the 512^3 sweep fields, for profilers: 2 untimed calls, then
+    --iters timed calls.  --profile-op is lap2|lap4|grad2|grad4|div2|div4."""
+    import torch
+    import pde_module_b200 as P
+    op, order = args.profile_op[:-1], int(args.profile_op[-1])
+    n = args.profile_n
+    g = order // 2
+    s = n + 2 * g
+    dx = 1.0 / n
+    fast = args.profile_fast
+    if op == "div":
+        u = torch.randn((s, s, s, 3), device="cuda")
+        m = P.Divergence(3, u.shape, dx, g, order=order, fast=fast)
+    elif op == "grad":
+        u = torch.randn((s, s, s, 1), device="cuda")
+        m = P.Grad(1, u.shape, dx, g, order=order, fast=fast)
+    else:
+        u = torch.randn((s, s, s, 1), device="cuda")
+        m = P.Laplacian(1, dx, g, order=order, fast=fast)
+    for _ in range(2):
+        m(u, 1.0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.iters):
+        m(u, 1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.iters
+    b = {"lap": 8, "grad": 16, "div": 16}[op]
+    print(json.dumps({"profile_op": args.profile_op, "n": n, "ms": ms, "gbs": n ** 3 * b / ms / 1e6}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -507,9 +542,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-heat", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the library's default tile candidates")
+    ap.add_argument("--profile-op", default=None, help="run one operator only (lap2, grad4, div2, ...)")
+    ap.add_argument("--profile-n", type=int, default=N_INT)
+    ap.add_argument("--profile-fast", action="store_true")
+    ap.add_argument("--iters", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_op:
+        return run_profile_op(args)
     return run_ours(args)
 
 
