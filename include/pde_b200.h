@@ -223,6 +223,30 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
                      int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
                      int32_t nsteps, int32_t steps_per_pass, void* stream);
 
+/* ---- fractional-step lid-driven cavity (new: the reference's LDC uses
+ * artificial compressibility, examples/LDC/LDC_Graph_Capture.py:71-90) ---- */
+typedef struct PdeLDCParams {
+  float   nu;               /* kinematic viscosity                              */
+  float   dt;               /* time step                                        */
+  int32_t jacobi_iters;     /* pressure sweeps per step                         */
+  int32_t jacobi_per_pass;  /* sweeps per launch (temporal blocking), 0 = 10    */
+} PdeLDCParams;
+
+/* nsteps of the projection method on a 2D grid, u (X,Y,1,2) and p (X,Y,1,1)
+ * advanced in place, composed of the reference operators in float32, one
+ * rounding per product and sum:
+ *   u2 = BC_u(u); u* = u2 + dt*(nu*Lap(u2) - Grad(u2) u2)
+ *   rhs = (1/dt)*Div(BC_u(u*))
+ *   jacobi_iters times: p <- 0.25*(pW + pE + pS + pN - dx^2*rhs) on BC_p(p)
+ *   u = BC_u(u*) + dt*(-Grad(BC_p(p)))
+ * u_rules / p_rules: compiled boundary groups (pde_bc_compile) of the velocity
+ * (2 components) and pressure (1).  u_star, p_tmp, rhs: scratch of u's, p's and
+ * p's size.  resid: device array of nsteps floats (or NULL) receiving the sum of
+ * squared pressure updates of each step's last sweep. */
+int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid,
+                    const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
+                    const PdeLDCParams* params, int32_t nsteps, void* stream);
+
 /* Allocation-free variant of pde_heat_rollout.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a memory manager
  * owns every allocation, cudaMalloc is not allowed in a latency-critical loop,

@@ -289,3 +289,39 @@ def stencil_at(u: np.ndarray, cells: np.ndarray, w: np.ndarray, axes_comps, alph
             idx[:, a] += t - R
             acc = acc + w[t] * u[idx[:, 0], idx[:, 1], idx[:, 2], comp]
     return dtype(alpha) * acc
+
+
+# ------------------------------------------------- fractional-step cavity ---
+def ldc_step(u, p, u_groups, p_groups, dx, ghost, nu, dt, jacobi_iters, dtype=np.float32):
+    """One projection step composed of the reference operators (no reference
+    counterpart: its cavity uses artificial compressibility,
+    examples/LDC/LDC_Graph_Capture.py:71-90).  u (X,Y,1,2), p (X,Y,1,1).
+
+        u2 = BC_u(u); u* = u2 + dt*(nu*Lap(u2) - Grad(u2) u2)
+        rhs = (1/dt)*Div(BC_u(u*))
+        jacobi_iters x: p <- 0.25*(pW + pE + pS + pN - dx^2*rhs) on BC_p(p)
+        u = BC_u(u*) + dt*Grad(BC_p(p), -1)
+    """
+    u2 = bc_apply(u, u_groups, dx, ghost, dtype=dtype)
+    lap = laplacian(u2, dx, ghost, nu, dtype=dtype)
+    G = grad(u2, dx, ghost, 1.0, dtype=dtype)  # (X,Y,1,2,2): row = component, column = axis
+    conv = G[..., 0] * u2[..., 0:1] + G[..., 1] * u2[..., 1:2]
+    us = forward_euler(u2, lap - conv, dt, dtype)
+    us_bc = bc_apply(us, u_groups, dx, ghost, dtype=dtype)
+    dt32 = float(np.float32(dt))
+    inv_dt = float(np.float32(1.0 / dt32)) if dtype == np.float32 else 1.0 / dt
+    rhs = divergence(us_bc, dx, ghost, inv_dt, dtype=dtype)
+    h2 = dtype(dx * dx)
+    X, Y = u.shape[0], u.shape[1]
+    c = (slice(ghost, X - ghost), slice(ghost, Y - ghost), 0, 0)
+    for _ in range(jacobi_iters):
+        pb = bc_apply(p, p_groups, dx, ghost, dtype=dtype)
+        new = pb.copy()
+        s = ((pb[ghost - 1:X - ghost - 1, ghost:Y - ghost, 0, 0] + pb[ghost + 1:X - ghost + 1, ghost:Y - ghost, 0, 0])
+             + pb[ghost:X - ghost, ghost - 1:Y - ghost - 1, 0, 0]) + pb[ghost:X - ghost, ghost + 1:Y - ghost + 1, 0, 0]
+        new[c] = dtype(0.25) * (s - h2 * rhs[c])
+        p = new
+    pb = bc_apply(p, p_groups, dx, ghost, dtype=dtype)
+    gp = grad(pb, dx, ghost, -1.0, dtype=dtype)
+    u_new = forward_euler(us_bc, gp, dt, dtype)
+    return u_new, p

@@ -68,6 +68,10 @@ class PdeBCRules(C.Structure):
     ]
 
 
+class PdeLDCParams(C.Structure):
+    _fields_ = [("nu", C.c_float), ("dt", C.c_float), ("jacobi_iters", C.c_int32), ("jacobi_per_pass", C.c_int32)]
+
+
 class PdeError(RuntimeError):
     """A C-ABI call returned a negative status."""
 
@@ -101,6 +105,9 @@ _SIGS = {
     "pde_heat_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                    C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                    C.c_void_p]),
+    "pde_ldc_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.POINTER(PdeBCRules),
+                                  C.POINTER(PdeLDCParams), C.c_int32, C.c_void_p]),
     "pde_heat_rollout_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                            C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                            C.c_void_p]),

@@ -69,6 +69,15 @@ __device__ __forceinline__ float bc_eval(const Geo& G, const PdeBCRules& Rl, con
   return U(c0, c1, c2, v);
 }
 
+// u2 at a cell of a 2D grid: cells strictly inside the node ring are neither
+// boundary nodes nor ghosts, so their boundary-filled value is the input value.
+template <class Acc>
+__device__ __forceinline__ float bc_eval2d(const Geo& G, const PdeBCRules& Rl, const Acc& U, int64_t i, int64_t j,
+                                           int v) {
+  if (i > G.g && i < G.n[0] - 1 - G.g && j > G.g && j < G.n[1] - 1 - G.g) return U(i, j, 0, v);
+  return bc_eval(G, Rl, U, i, j, 0, v);
+}
+
 struct GlobalAcc {
   const float* u;
   int64_t s0, s1;  // cell strides
@@ -214,45 +223,46 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
   const int RX = rx1 - rx0, RY = ry1 - ry0;
   float* A = sm;
   float* B = sm + P.RXM * P.RYM * N;
-  const int nrow = RY * N, ncell = RX * nrow;
-  for (int idx = threadIdx.x; idx < ncell; idx += blockDim.x) {
-    const int lx = idx / nrow, rem = idx - lx * nrow;
-    A[idx] = __ldg(in + ((size_t)(rx0 + lx) * P.Y + ry0) * N + rem);
-  }
+  const int nrow = RY * N;  // floats per region row
+  // 2D thread layout: 32 lanes along the contiguous (y, component) floats, blockDim.x / 32 rows
+  const int lf0 = threadIdx.x & 31, lx0 = threadIdx.x >> 5, nrows = blockDim.x >> 5;
+  for (int lx = lx0; lx < RX; lx += nrows)
+    for (int lf = lf0; lf < nrow; lf += 32) A[lx * nrow + lf] = __ldg(in + ((size_t)(rx0 + lx) * P.Y + ry0) * N + lf);
   __syncthreads();
   const int g = P.g;
+  // stencil cells whose R neighbours along both axes are inside the region
+  const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(P.X - g, rx0 + RX - R) - rx0;
+  const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(P.Y - g, ry0 + RY - R) - ry0;
   for (int s = 0; s < P.k; ++s) {
     bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY);
-    for (int idx = threadIdx.x; idx < ncell; idx += blockDim.x) {
-      const int lx = idx / nrow, rem = idx - lx * nrow;
-      const int ly = rem / N;
-      const int x = rx0 + lx, y = ry0 + ly;
-      const float u2 = A[idx];
-      float res = u2;
-      if (x >= g && x < P.X - g && y >= g && y < P.Y - g && lx >= R && lx < RX - R && ly >= R && ly < RY - R) {
-        float acc = 0.0f;
+    for (int lx = lx0; lx < RX; lx += nrows)
+      for (int lf = lf0; lf < nrow; lf += 32) {
+        const int idx = lx * nrow + lf;
+        const int ly = lf / N;
+        const float u2 = A[idx];
+        float res = u2;
+        if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
+          float acc = 0.0f;
 #pragma unroll
-        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * nrow]));
+          for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * nrow]));
 #pragma unroll
-        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * N]));
-        res = add(u2, mul(P.dt, mul(P.alpha, acc)));
+          for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * N]));
+          res = add(u2, mul(P.dt, mul(P.alpha, acc)));
+        }
+        B[idx] = res;
       }
-      B[idx] = res;
-    }
     __syncthreads();
     float* tmp = A;
     A = B;
     B = tmp;
   }
-  // The ghost cells of the result hold the last step's boundary-filled values,
-  // which B (the pre-step buffer) already has; A holds u2 copied through.
+  // The ghost cells of the result hold the last step's boundary-filled values
+  // (non-stencil cells copy their filled value through).
   const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
-  const int onrow = (oy1 - by0) * N, on = (ox1 - bx0) * onrow;
-  for (int idx = threadIdx.x; idx < on; idx += blockDim.x) {
-    const int lx = idx / onrow, rem = idx - lx * onrow;
-    const int x = bx0 + lx;
-    out[((size_t)x * P.Y + by0) * N + rem] = A[((x - rx0) * RY + (by0 - ry0)) * N + rem];
-  }
+  const int onrow = (oy1 - by0) * N;
+  for (int lx = lx0; lx < ox1 - bx0; lx += nrows)
+    for (int lf = lf0; lf < onrow; lf += 32)
+      out[((size_t)(bx0 + lx) * P.Y + by0) * N + lf] = A[(bx0 + lx - rx0) * nrow + (by0 - ry0) * N + lf];
 }
 
 }  // namespace pde

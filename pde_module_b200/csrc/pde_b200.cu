@@ -8,6 +8,7 @@
 #include "generic.cuh"
 #include "stream3d.cuh"
 #include "fused.cuh"
+#include "ldc.cuh"
 
 using namespace pde;
 
@@ -528,6 +529,64 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
     dst = (dst == work) ? u_out : work;
   }
   if (need_copy) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, work, bytes, cudaMemcpyDeviceToDevice, st));
+  return PDE_OK;
+}
+
+int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid, const PdeGrid* grid,
+                    const PdeBCRules* u_rules, const PdeBCRules* p_rules, const PdeLDCParams* prm, int32_t nsteps,
+                    void* stream) {
+  if (!u || !p || !u_star || !p_tmp || !rhs || !grid || !u_rules || !p_rules || !prm || nsteps < 0)
+    return PDE_ERR_ARG;
+  if (u_rules->ncomp != 2 || p_rules->ncomp != 1 || u_rules->has_ramp || p_rules->has_ramp) return PDE_ERR_ARG;
+  if (prm->jacobi_iters < 0 || prm->jacobi_per_pass < 0) return PDE_ERR_ARG;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  if (G.ndims != 2 || G.n[2] != 1 || grid->order != 2) return PDE_ERR_UNSUPPORTED;
+  if (G.g < 1) return PDE_ERR_GHOST;
+  cudaStream_t st = as_stream(stream);
+  const Weights WL = lap_weights(2, grid->dx), WD = d1_weights(2, grid->dx);
+  LdcConst K;
+  for (int t = 0; t < 3; ++t) { K.wl[t] = WL.w[t]; K.wd[t] = WD.w[t]; }
+  K.nu = prm->nu;
+  K.dt = prm->dt;
+  K.inv_dt = (float)(1.0 / (double)prm->dt);
+  K.h2 = (float)(grid->dx * grid->dx);
+  const int64_t cells = G.n[0] * G.n[1];
+  const int blocks = grid_blocks(cells, 256);
+  if (resid && nsteps > 0) PDE_CUDA_CHECK(cudaMemsetAsync(resid, 0, sizeof(float) * nsteps, st));
+  const int iters = prm->jacobi_iters;
+  int k = prm->jacobi_per_pass > 0 ? prm->jacobi_per_pass : 10;
+  if (k > iters && iters > 0) k = iters;
+  J2Params JP;
+  JP.X = (int)G.n[0]; JP.Y = (int)G.n[1]; JP.g = G.g;
+  JP.TBX = 32; JP.TBY = 64;
+  JP.tiles_y = (JP.Y + JP.TBY - 1) / JP.TBY;
+  JP.RXM = JP.TBX + 2 * (k + 1);
+  JP.RYM = JP.TBY + 2 * (k + 1);
+  JP.h2 = K.h2;
+  const int jtiles = ((JP.X + JP.TBX - 1) / JP.TBX) * JP.tiles_y;
+  const size_t jsmem = (size_t)3 * JP.RXM * JP.RYM * sizeof(float);
+  if (jsmem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(jacobi2d_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem));
+  for (int step = 0; step < nsteps; ++step) {
+    ldc_predictor_kernel<<<blocks, 256, 0, st>>>(u, u_star, G, *u_rules, K);
+    ldc_divergence_kernel<<<blocks, 256, 0, st>>>(u_star, rhs, G, *u_rules, K);
+    float* src = p;
+    float* dst = p_tmp;
+    for (int done = 0; done < iters;) {
+      JP.k = (iters - done < k) ? (iters - done) : k;
+      done += JP.k;
+      JP.last = (done == iters);
+      jacobi2d_tb_kernel<<<jtiles, 256, jsmem, st>>>(src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
+      float* t = src;
+      src = dst;
+      dst = t;
+    }
+    if (src != p) PDE_CUDA_CHECK(cudaMemcpyAsync(p, src, sizeof(float) * cells, cudaMemcpyDeviceToDevice, st));
+    ldc_project_kernel<<<blocks, 256, 0, st>>>(u_star, p, u, G, *u_rules, *p_rules, K);
+    const int rc = launch_status();
+    if (rc) return rc;
+  }
   return PDE_OK;
 }
 

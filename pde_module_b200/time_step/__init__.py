@@ -1,2 +1,3 @@
 from .forwardEuler import ForwardEuler
 from .heat import HeatRollout
+from .fractional_step import FractionalStepLDC
