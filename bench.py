@@ -327,6 +327,9 @@ def run_ours(args):
     ldc = None
     if rank == 0 and not args.no_ldc:
         ldc = run_ldc()
+    wave = None
+    if rank == 0 and not args.no_wave:
+        wave = run_wave()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -353,6 +356,7 @@ def run_ours(args):
                                   "exact mode, bit-identical to the reference algorithm"},
             "heat_256": heat,
             "ldc_1024": ldc,
+            "wave_512": wave,
             "autotune": {f"{k[0]}_n{k[1]}_o{k[2]}": v for k, v in tuned.items()},
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * len(ops), "clocks": clocks,
@@ -499,6 +503,67 @@ def run_ldc(steps: int = 2000, n: int = 1024):
             "note": "L2-resident (about 28 MB of fields); CUDA graph replay of the whole rollout"}
 
 
+def run_wave(n: int = 512, steps: int = 2000):
+    """Differentiable wave, n^2 nodes, leapfrog at CFL 0.5, Ricker source, MSE loss
+    against a target from another speed field; gradients w.r.t. the speed field and the
+    initial field through the adjoint with sqrt(N) checkpoints.  Times the forward
+    rollout and forward + adjoint."""
+    import torch
+    from pde_module_b200.time_step import wave as W
+    solver, c, u0, target, dt, mask = W.make_problem(n=n, nsteps=steps)
+
+    def fwd_only():
+        with torch.no_grad():
+            return W.wave_rollout((dt * dt) * c * c, u0, solver)
+
+    def fwd_adj():
+        cc = c.clone().requires_grad_(True)
+        uu = u0.clone().requires_grad_(True)
+        uN = W.wave_rollout((dt * dt) * cc * cc, uu, solver)
+        loss = (((uN - target) * mask) ** 2).sum() / mask.sum()
+        loss.backward()
+        return loss, cc.grad, uu.grad
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, out
+
+    best = None
+    for k in (4, 8, 12, 16):
+        solver.steps_per_pass = k
+        ms, _ = timed(fwd_adj, 1)
+        if best is None or ms < best[0]:
+            best = (ms, k)
+    solver.steps_per_pass = best[1]
+    f_ms, _ = timed(fwd_only)
+    fa_ms, (loss, gc, gu) = timed(fwd_adj)
+    # the same with every state kept (one segment: no recomputation; 2000 x 1 MB)
+    every = solver.every
+    solver.every = steps
+    solver._work = None
+    fa_all_ms, (loss2, gc2, _) = timed(fwd_adj)
+    solver.every = every
+    solver._work = None
+    same = bool(torch.equal(gc, gc2))
+    cells = n * n * steps
+    return {"workload": f"differentiable wave {n}^2, {steps} leapfrog steps, CFL 0.5, Ricker source, "
+                        f"MSE vs target, grads w.r.t. speed and initial field, sqrt(N) checkpoints "
+                        f"(every {solver.every} steps)",
+            "forward_ms": f_ms, "forward_adjoint_ms": fa_ms, "ratio_fwd_adj_over_fwd": fa_ms / f_ms,
+            "store_all_states": {"forward_adjoint_ms": fa_all_ms, "ratio_fwd_adj_over_fwd": fa_all_ms / f_ms,
+                                 "grad_bitwise_equal_to_checkpointed": same},
+            "forward_cell_updates_per_s": cells / (f_ms / 1000.0), "steps_per_pass": best[1],
+            "loss": float(loss.item()), "grad_c_norm": float(gc.norm().item()),
+            "grad_u0_norm": float(gu.norm().item())}
+
+
 def run_e2e(fields, ops, world, args):
     import torch
     import torch.distributed as dist
@@ -592,6 +657,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-heat", action="store_true")
     ap.add_argument("--no-ldc", action="store_true")
+    ap.add_argument("--no-wave", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the library's default tile candidates")
     ap.add_argument("--profile-op", default=None, help="run one operator only (lap2, grad4, div2, ...)")
     ap.add_argument("--profile-n", type=int, default=N_INT)

@@ -247,6 +247,27 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
                     const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
                     const PdeLDCParams* params, int32_t nsteps, void* stream);
 
+/* ---- differentiable 2D wave equation (new; the reference's wave examples step a
+ * first-order (u, v) pair with forward Euler, tests/FDM/test_WaveStanding.py:71-76) ----
+ * State on the cells strictly inside the Dirichlet node ring (nodes and ghosts 0),
+ * K = dt^2 c^2 a field, L the 5-point Laplacian in the reference's order:
+ *   u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) + src[n] at src_cell
+ * pde_wave_forward: nsteps from (u^{n0-1}, u^{n0}) = (u_prev, u_cur) to
+ * (out_prev, out_cur) = (u^{n0+nsteps-1}, u^{n0+nsteps}); src_cell < 0: no source.
+ * states (NULL or nsteps fields): states[j] = u^{n0+1+j}.  work: 2 fields.
+ * steps_per_pass: temporal-blocking depth (0 = 8). */
+int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, float* out_prev, float* out_cur,
+                     const float* src, int64_t src_cell, int32_t n0, int32_t nsteps, int32_t steps_per_pass,
+                     float* states, float* work, const PdeGrid* grid, void* stream);
+/* Discrete adjoint over steps n = nsteps-1 .. 0 of a segment whose states are
+ * ustates[j] = u^j (j = 0 .. nsteps-1):  mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1}),
+ * grad_K += mu^{n+1} o L(u^n) (read-modify-write once per step, n descending).
+ * In: (mu_next, mu_next2) = (mu^{nsteps}, mu^{nsteps+1}); out: (mu_out, mu_out_next) =
+ * (mu^0, mu^1).  work: 2 fields. */
+int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out,
+                     float* mu_out_next, const float* ustates, float* grad_K, int32_t nsteps,
+                     int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
+
 /* Allocation-free variant of pde_heat_rollout.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a memory manager
  * owns every allocation, cudaMalloc is not allowed in a latency-critical loop,

@@ -325,3 +325,66 @@ def ldc_step(u, p, u_groups, p_groups, dx, ghost, nu, dt, jacobi_iters, dtype=np
     gp = grad(pb, dx, ghost, -1.0, dtype=dtype)
     u_new = forward_euler(us_bc, gp, dt, dtype)
     return u_new, p
+
+
+# ------------------------------------------------------ differentiable wave ---
+def _wave_interior(X, Y, ghost):
+    m = np.zeros((X, Y), dtype=bool)
+    m[ghost + 1:X - 1 - ghost, ghost + 1:Y - 1 - ghost] = True
+    return m
+
+
+def _lap5(u, w, dtype):
+    """5-point Laplacian (reference order, alpha 1) at every cell not on the array edge."""
+    out = np.zeros_like(u)
+    c = u[1:-1, 1:-1]
+    acc = dtype(0) + w[0] * u[:-2, 1:-1]
+    acc = acc + w[1] * c
+    acc = acc + w[2] * u[2:, 1:-1]
+    acc = acc + w[0] * u[1:-1, :-2]
+    acc = acc + w[1] * c
+    acc = acc + w[2] * u[1:-1, 2:]
+    out[1:-1, 1:-1] = acc
+    return out
+
+
+def wave_forward(K, u0, src, src_cell, nsteps, dx, ghost=1, dtype=np.float32):
+    """New (no reference counterpart).  Leapfrog on the cells strictly inside the
+    node ring: u^{n+1} = 2u^n - u^{n-1} + K o L(u^n) + src[n] at src_cell,
+    u^{-1} = u^0 = u0.  K, u0: (X, Y, 1, 1).  Returns [u^0, ..., u^N] as (X, Y) arrays."""
+    K2 = np.asarray(K, dtype=dtype)[:, :, 0, 0]
+    X, Y = K2.shape
+    I = _wave_interior(X, Y, ghost)
+    w = lap_weights(2, dx, dtype)
+    u = np.where(I, np.asarray(u0, dtype=dtype)[:, :, 0, 0], dtype(0))
+    um = u.copy()
+    sx, sy = (src_cell // Y, src_cell % Y) if src_cell is not None and src_cell >= 0 else (-1, -1)
+    states = [u]
+    for n in range(nsteps):
+        v = dtype(2.0) * u - um
+        v = v + K2 * _lap5(u, w, dtype)
+        if sx >= 0:
+            v[sx, sy] = v[sx, sy] + dtype(src[n])
+        v = np.where(I, v, dtype(0))
+        um, u = u, v
+        states.append(u)
+    return states
+
+
+def wave_adjoint(K, states, muN, dx, ghost=1, dtype=np.float32):
+    """Discrete adjoint of wave_forward: mu^n = 2mu^{n+1} - mu^{n+2} + L(K o mu^{n+1}),
+    dJ/dK += mu^{n+1} o L(u^n) for n = N-1 .. 0.  Returns (dJ/dK, mu^0, mu^1) as (X, Y)."""
+    K2 = np.asarray(K, dtype=dtype)[:, :, 0, 0]
+    X, Y = K2.shape
+    I = _wave_interior(X, Y, ghost)
+    w = lap_weights(2, dx, dtype)
+    mu1 = np.where(I, np.asarray(muN, dtype=dtype)[:, :, 0, 0], dtype(0))
+    mu2 = np.zeros_like(mu1)
+    gK = np.zeros_like(mu1)
+    for n in range(len(states) - 2, -1, -1):
+        gK = np.where(I, gK + mu1 * _lap5(states[n], w, dtype), gK)
+        mu0 = dtype(2.0) * mu1 - mu2
+        mu0 = mu0 + _lap5(K2 * mu1, w, dtype)
+        mu0 = np.where(I, mu0, dtype(0))
+        mu2, mu1 = mu1, mu0
+    return gK, mu1, mu2

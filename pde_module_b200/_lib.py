@@ -108,6 +108,11 @@ _SIGS = {
     "pde_ldc_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.POINTER(PdeBCRules),
                                   C.POINTER(PdeLDCParams), C.c_int32, C.c_void_p]),
+    "pde_wave_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                   C.POINTER(PdeGrid), C.c_void_p]),
+    "pde_wave_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(PdeGrid), C.c_void_p]),
     "pde_heat_rollout_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                            C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                            C.c_void_p]),

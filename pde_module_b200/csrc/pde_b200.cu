@@ -9,6 +9,7 @@
 #include "stream3d.cuh"
 #include "fused.cuh"
 #include "ldc.cuh"
+#include "wave.cuh"
 
 using namespace pde;
 
@@ -529,6 +530,135 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
     dst = (dst == work) ? u_out : work;
   }
   if (need_copy) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, work, bytes, cudaMemcpyDeviceToDevice, st));
+  return PDE_OK;
+}
+
+namespace {
+
+bool wave_setup(const PdeGrid* grid, int steps_per_pass, int nsteps, Geo* G, WaveParams* P, int* kk, size_t* smem,
+                int nbuf) {
+  if (!make_geo(grid, G)) return false;
+  if (G->ndims != 2 || G->n[2] != 1 || grid->order != 2 || G->g < 1) return false;
+  const Weights WL = lap_weights(2, grid->dx);
+  memset(P, 0, sizeof(*P));
+  P->X = (int)G->n[0];
+  P->Y = (int)G->n[1];
+  P->g = G->g;
+  for (int t = 0; t < 3; ++t) P->w[t] = WL.w[t];
+  int k = steps_per_pass > 0 ? steps_per_pass : 8;
+  if (k > nsteps) k = nsteps;
+  if (k < 1) k = 1;
+  *kk = k;
+  P->TBX = WAVE_TBX;
+  P->TBY = WAVE_TBY;
+  P->tiles_y = (P->Y + P->TBY - 1) / P->TBY;
+  P->RXM = P->TBX + 2 * k;
+  P->RYM = P->TBY + 2 * k;
+  P->cells = (long long)G->n[0] * G->n[1];
+  P->srcx = -1;
+  *smem = (size_t)nbuf * P->RXM * P->RYM * sizeof(float);
+  return *smem <= 227 * 1024;
+}
+
+}  // namespace
+
+int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, float* out_prev, float* out_cur,
+                     const float* src, int64_t src_cell, int32_t n0, int32_t nsteps, int32_t steps_per_pass,
+                     float* states, float* work, const PdeGrid* grid, void* stream) {
+  if (!K || !u_prev || !u_cur || !out_prev || !out_cur || !work || !grid || nsteps < 0 || n0 < 0) return PDE_ERR_ARG;
+  if (src_cell >= 0 && !src) return PDE_ERR_ARG;
+  Geo G;
+  WaveParams P;
+  int k;
+  size_t smem;
+  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 4)) return PDE_ERR_UNSUPPORTED;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = sizeof(float) * (size_t)P.cells;
+  if (nsteps == 0) {
+    if (out_prev != u_prev) PDE_CUDA_CHECK(cudaMemcpyAsync(out_prev, u_prev, bytes, cudaMemcpyDeviceToDevice, st));
+    if (out_cur != u_cur) PDE_CUDA_CHECK(cudaMemcpyAsync(out_cur, u_cur, bytes, cudaMemcpyDeviceToDevice, st));
+    return PDE_OK;
+  }
+  if (src_cell >= P.cells) return PDE_ERR_ARG;
+  if (src_cell >= 0) {
+    P.srcx = (int)(src_cell / P.Y);
+    P.srcy = (int)(src_cell % P.Y);
+    P.src = src;
+  }
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_fwd_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  const int npasses = (nsteps + k - 1) / k;
+  float* w0 = work;
+  float* w1 = work + P.cells;
+  const bool alias = out_prev == u_prev || out_cur == u_cur || out_prev == u_cur || out_cur == u_prev;
+  bool to_out = alias ? false : (npasses % 2 == 1);
+  const float* a = u_prev;
+  const float* b = u_cur;
+  int done = 0;
+  for (int p = 0; p < npasses; ++p) {
+    P.k = (nsteps - done < k) ? (nsteps - done) : k;
+    P.n0 = n0 + done;
+    P.states = states ? states + (size_t)done * P.cells : nullptr;
+    float* da = to_out ? out_prev : w0;
+    float* db = to_out ? out_cur : w1;
+    wave_fwd_tb_kernel<<<tiles, 256, smem, st>>>(a, b, K, da, db, P);
+    const int rc = launch_status();
+    if (rc) return rc;
+    a = da;
+    b = db;
+    done += P.k;
+    to_out = !to_out;
+  }
+  if (a != out_prev) {
+    PDE_CUDA_CHECK(cudaMemcpyAsync(out_prev, a, bytes, cudaMemcpyDeviceToDevice, st));
+    PDE_CUDA_CHECK(cudaMemcpyAsync(out_cur, b, bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  return PDE_OK;
+}
+
+int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out, float* mu_out_next,
+                     const float* ustates, float* grad_K, int32_t nsteps, int32_t steps_per_pass, float* work,
+                     const PdeGrid* grid, void* stream) {
+  if (!K || !mu_next || !mu_next2 || !mu_out || !mu_out_next || !ustates || !grad_K || !work || !grid ||
+      nsteps < 1)
+    return PDE_ERR_ARG;
+  Geo G;
+  WaveParams P;
+  int k;
+  size_t smem;
+  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 4)) return PDE_ERR_UNSUPPORTED;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = sizeof(float) * (size_t)P.cells;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_adj_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  const int npasses = (nsteps + k - 1) / k;
+  float* w0 = work;
+  float* w1 = work + P.cells;
+  const bool alias = mu_out == mu_next || mu_out_next == mu_next2 || mu_out == mu_next2 || mu_out_next == mu_next;
+  bool to_out = alias ? false : (npasses % 2 == 1);
+  const float* a = mu_next;
+  const float* b = mu_next2;
+  P.ustates = ustates;
+  P.ubase = 0;  // ustates[j] = u^{nbot + j}; steps are numbered from nbot = 0 here
+  P.gK = grad_K;
+  int done = 0;
+  for (int p = 0; p < npasses; ++p) {
+    P.k = (nsteps - done < k) ? (nsteps - done) : k;
+    P.ntop = nsteps - 1 - done;
+    float* da = to_out ? mu_out : w0;
+    float* db = to_out ? mu_out_next : w1;
+    wave_adj_tb_kernel<<<tiles, 256, smem, st>>>(a, b, K, da, db, P);
+    const int rc = launch_status();
+    if (rc) return rc;
+    a = da;
+    b = db;
+    done += P.k;
+    to_out = !to_out;
+  }
+  if (a != mu_out) {
+    PDE_CUDA_CHECK(cudaMemcpyAsync(mu_out, a, bytes, cudaMemcpyDeviceToDevice, st));
+    PDE_CUDA_CHECK(cudaMemcpyAsync(mu_out_next, b, bytes, cudaMemcpyDeviceToDevice, st));
+  }
   return PDE_OK;
 }
 
