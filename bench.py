@@ -330,6 +330,9 @@ def run_ours(args):
     wave = None
     if rank == 0 and not args.no_wave:
         wave = run_wave()
+    batched = None
+    if rank == 0 and not args.no_batched:
+        batched = run_batched(tune=not args.no_tune)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -357,6 +360,7 @@ def run_ours(args):
             "heat_256": heat,
             "ldc_1024": ldc,
             "wave_512": wave,
+            "batched_64": batched,
             "autotune": {f"{k[0]}_n{k[1]}_o{k[2]}": v for k, v in tuned.items()},
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * len(ops), "clocks": clocks,
@@ -564,6 +568,155 @@ def run_wave(n: int = 512, steps: int = 2000):
             "grad_u0_norm": float(gu.norm().item())}
 
 
+def batched_problem(n_grids: int = 64, lo: int = 64, hi: int = 1024):
+    """64 independent 2D grids: interior sides from rng(3).integers(64, 1025, (64, 2)),
+    diffusivity exp(U[ln 1e-3, 0]) from rng(4), u0 = U[0,1) from rng(5 + i), one ghost
+    layer, dx = 1 / max(side), dt = 0.2 dx^2 / alpha."""
+    sides = np.random.default_rng(3).integers(lo, hi + 1, size=(n_grids, 2))
+    alpha = np.exp(np.random.default_rng(4).uniform(np.log(1e-3), 0.0, size=n_grids))
+    u0, dx, dt = [], [], []
+    for i, (sx, sy) in enumerate(sides):
+        u0.append(np.random.default_rng(5 + i).random((int(sx) + 2, int(sy) + 2)).astype(np.float32))
+        h = 1.0 / int(max(sx, sy))
+        dx.append(h)
+        dt.append(0.2 * h * h / float(alpha[i]))
+    return sides, alpha.tolist(), u0, dx, dt
+
+
+def run_batched(steps: int = 500, chain_steps: int = 50, tune: bool = True):
+    """Batched heat and wave rollouts of 64 uneven grids in one persistent launch
+    (replayed as a CUDA graph), against per-grid plain launches: the module chain
+    GridBoundary -> Laplacian -> ForwardEuler of examples/2D_Heat_Equation.py per grid
+    and step (captured as a CUDA graph over chain_steps steps; the time is linear in
+    steps and is scaled to the rollout's), and per-grid fused rollouts."""
+    import torch
+    import pde_module_b200 as P
+    from pde_module_b200 import tuning
+    sides, alpha, u0, dx, dt = batched_problem()
+    n = len(u0)
+    interior = int(sum(int(a) * int(b) for a, b in sides))
+    cells_arr = int(sum(u.size for u in u0))
+    dev0 = [torch.from_numpy(u[:, :, None, None]).cuda() for u in u0]
+
+    def graph_of(fn):
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            fn()
+            gph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gph, stream=s):
+                fn()
+        torch.cuda.current_stream().wait_stream(s)
+        return gph
+
+    def timed(gph, reps=3):
+        gph.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            gph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": f"batched heat: {n} 2D grids, interior sides U{{64..1024}} (rng 3), alpha log-uniform "
+                       f"[1e-3, 1] (rng 4), u0 U[0,1) (rng 5+i), Dirichlet 0, dt = 0.2 dx^2/alpha, {steps} steps",
+           "grids": n, "interior_cells": interior, "array_cells": cells_arr}
+    # --- batched heat -----------------------------------------------------------
+    fields = [u.clone() for u in dev0]
+    roll = P.BatchedHeatRollout(fields, dx, alpha, dt)
+    if tune:
+        t = tuning.tune_batched(roll, nsteps=100)
+        out["autotune"] = {"best": list(t["best"]), "ms_100_steps": t["ms"]}
+    for f, u in zip(fields, dev0):
+        f.copy_(u)
+    g_b = graph_of(lambda: roll(steps))
+    b_ms = timed(g_b)
+    # parity: a fresh rollout against per-grid fused rollouts (bitwise)
+    for f, u in zip(fields, dev0):
+        f.copy_(u)
+    g_b.replay()
+    torch.cuda.synchronize()
+    err = P._lib.device_error()
+    bcs = []
+    for i in range(n):
+        bc = P.GridBoundary(dev0[i], dx[i], 1)
+        bc.dirichlet_BC("ALL", 0.0)
+        bcs.append(bc)
+    rolls = [P.HeatRollout(bcs[i], dx[i], alpha[i], dt[i], steps_per_pass=8) for i in range(n)]
+    same = all(torch.equal(rolls[i](dev0[i], steps), fields[i]) for i in range(n))
+    g_pg = graph_of(lambda: [rolls[i](dev0[i], steps) for i in range(n)])
+    pg_ms = timed(g_pg)
+    # per-grid module chain, chain_steps steps per replay
+    laps = [P.Laplacian(1, dx[i], 1) for i in range(n)]
+    eulers = [P.ForwardEuler() for _ in range(n)]
+
+    def chain():
+        for i in range(n):
+            u = dev0[i]
+            for _ in range(chain_steps):
+                u2 = bcs[i](u)
+                u = eulers[i](u2, laps[i](u2, alpha[i]), dt[i])
+
+    g_c = graph_of(chain)
+    c_ms = timed(g_c, reps=2) * (steps / chain_steps)
+    del g_c
+    upd = interior * steps
+    out["heat"] = {"batched_ms": b_ms, "batched_cell_updates_per_s": upd / (b_ms / 1000.0),
+                   "plain_chain_ms": c_ms, "plain_chain_cell_updates_per_s": upd / (c_ms / 1000.0),
+                   "per_grid_fused_ms": pg_ms, "per_grid_fused_cell_updates_per_s": upd / (pg_ms / 1000.0),
+                   "speedup_vs_plain_chain": c_ms / b_ms, "speedup_vs_per_grid_fused": pg_ms / b_ms,
+                   "tile": [roll.plan.tile_x, roll.plan.tile_y], "steps_per_pass": roll.plan.steps_per_pass,
+                   "persistent_blocks": roll.plan.blocks, "total_tiles": roll.plan.total_tiles,
+                   "hbm_bytes_algorithmic": 8 * cells_arr * (-(-steps // roll.plan.steps_per_pass) +
+                                                             (-(-steps // roll.plan.steps_per_pass)) % 2),
+                   "bitwise_equal_to_per_grid": bool(same), "device_error": err,
+                   "note": "plain chain = per-grid GridBoundary, Laplacian, ForwardEuler launches, as a CUDA "
+                           f"graph of {chain_steps} steps x {n} grids scaled to {steps} steps"}
+    del g_b, g_pg
+    # --- batched wave: K = dt^2 c^2 = 0.125 dx^2 (CFL 0.5 in 2D), zero Dirichlet ring
+    wf = []
+    for u in u0:
+        w = u.copy()
+        w[:2, :] = 0.0; w[-2:, :] = 0.0; w[:, :2] = 0.0; w[:, -2:] = 0.0
+        wf.append(torch.from_numpy(w[:, :, None, None]).cuda())
+    Ks = [0.125 * h * h for h in dx]
+    cur = [w.clone() for w in wf]
+    prev = [w.clone() for w in wf]
+    wroll = P.BatchedWaveRollout(cur, prev, dx, Ks)
+    if tune:
+        t = tuning.tune_batched(wroll, nsteps=100)
+        out["wave_autotune"] = {"best": list(t["best"])}
+    for a, b, w in zip(cur, prev, wf):
+        a.copy_(w)
+        b.copy_(w)
+    g_w = graph_of(lambda: wroll(steps))
+    w_ms = timed(g_w)
+    for a, b, w in zip(cur, prev, wf):
+        a.copy_(w)
+        b.copy_(w)
+    g_w.replay()
+    from pde_module_b200.time_step.wave import WaveSolver
+    # per-grid fused forward rollouts (pde_wave_forward, no states kept), one call per grid
+    solvers = [WaveSolver(tuple(wf[i].shape[:3]), dx[i], steps, steps_per_pass=8, checkpoint_every=1)
+               for i in range(n)]
+    Kf = [torch.full_like(wf[i], Ks[i]) for i in range(n)]
+    wout = [(torch.empty_like(w), torch.empty_like(w)) for w in wf]
+    for i in range(n):
+        solvers[i]._buffers(Kf[i])
+    g_wp = graph_of(lambda: [solvers[i]._fwd(Kf[i], wf[i], wf[i], wout[i][0], wout[i][1], 0, steps)
+                             for i in range(n)])
+    wp_ms = timed(g_wp)
+    wsame = all(torch.equal(wout[i][1], cur[i]) for i in range(n))
+    out["wave"] = {"batched_ms": w_ms, "batched_cell_updates_per_s": upd / (w_ms / 1000.0),
+                   "per_grid_fused_ms": wp_ms, "speedup_vs_per_grid_fused": wp_ms / w_ms,
+                   "bitwise_equal_to_per_grid": bool(wsame),
+                   "tile": [wroll.plan.tile_x, wroll.plan.tile_y], "steps_per_pass": wroll.plan.steps_per_pass}
+    del g_w, g_wp
+    return out
+
+
 def run_e2e(fields, ops, world, args):
     import torch
     import torch.distributed as dist
@@ -658,6 +811,7 @@ def main():
     ap.add_argument("--no-heat", action="store_true")
     ap.add_argument("--no-ldc", action="store_true")
     ap.add_argument("--no-wave", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the library's default tile candidates")
     ap.add_argument("--profile-op", default=None, help="run one operator only (lap2, grad4, div2, ...)")
     ap.add_argument("--profile-n", type=int, default=N_INT)

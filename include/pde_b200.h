@@ -268,6 +268,58 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
                      float* mu_out_next, const float* ustates, float* grad_K, int32_t nsteps,
                      int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
 
+/* ---- batched rollouts (new: the reference advances every grid with its own
+ * module chain, examples/2D_Heat_Equation.py:57-65, three launches per step
+ * per grid).  Many independent 2D grids of uneven sizes advance together in
+ * ONE persistent launch over a tile work queue: items (time block, grid, tile)
+ * in time-block-major order; a tile starts a time block once its 3x3
+ * neighbours finished the previous one (bounded waits, PDE_ERR_TIMEOUT).
+ * Heat results are bit-identical to pde_heat_rollout per grid; wave results to
+ * pde_wave_forward with a constant K field and no source. ---- */
+#define PDE_BATCH_HEAT 0
+#define PDE_BATCH_WAVE 1
+
+typedef struct PdeBatchGrid {
+  float*  field;       /* heat: u; wave: u^n.  (X, Y, 1, 1) float32 incl. ghosts,
+                          overwritten by the result (u after nsteps; u^{n+nsteps}) */
+  float*  field_prev;  /* wave: u^{n-1}, overwritten by u^{n+nsteps-1}; heat: NULL  */
+  float*  scratch;     /* device scratch: X*Y floats (heat), 2*X*Y floats (wave)    */
+  int64_t shape[2];    /* X, Y including ghosts                                     */
+  double  dx;          /* spacing (Laplacian weights; heat Neumann ghosts)          */
+  float   coef;        /* heat: diffusivity alpha; wave: K = dt^2 c^2               */
+  float   dt;          /* heat: time step; wave: unused                             */
+} PdeBatchGrid;
+
+typedef struct PdeBatchPlan {
+  void*      table;           /* device: descriptors + queue state (in `work`)      */
+  int32_t    kind;            /* PDE_BATCH_HEAT or PDE_BATCH_WAVE                   */
+  int32_t    ngrids;
+  int32_t    total_tiles;
+  int32_t    ghost_cells;
+  int32_t    order;           /* heat: 2 or 4; wave: 2                              */
+  int32_t    tile_x, tile_y;  /* output tile (cells, ghosts included)               */
+  int32_t    steps_per_pass;  /* time-block depth k                                 */
+  int32_t    blocks;          /* persistent grid size                               */
+  int32_t    smem_bytes;
+  PdeBCRules rules;           /* heat: the boundary groups every grid shares        */
+} PdeBatchPlan;
+
+/* Device bytes `work` must hold for these grids and tile (0 = default). */
+int pde_batch_work_bytes(const PdeBatchGrid* grids, int32_t ngrids, int32_t tile_x, int32_t tile_y,
+                         uint64_t* bytes);
+/* Validate the grids, choose the launch (tile 0 = 32 x 64, steps_per_pass 0 =
+ * 8) and upload the descriptor table into `work` on `stream` (from pageable
+ * host memory: call it outside stream capture).  `rules` (heat only; compiled
+ * by pde_bc_compile for any grid of the batch, ncomp 1, constant values) is
+ * copied into the plan; each grid's own dx is used for its Neumann ghosts.
+ * The halo (heat k*R+1, wave k) may not exceed a tile side. */
+int pde_batch_plan(int32_t kind, const PdeBatchGrid* grids, int32_t ngrids, int32_t ghost_cells, int32_t order,
+                   const PdeBCRules* rules, int32_t tile_x, int32_t tile_y, int32_t steps_per_pass, void* work,
+                   uint64_t work_bytes, PdeBatchPlan* plan, void* stream);
+/* Advance every grid of the plan nsteps: one memset of the queue state and one
+ * kernel launch, so it can be captured in a CUDA graph. */
+int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream);
+
 /* Allocation-free variant of pde_heat_rollout.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a memory manager
  * owns every allocation, cudaMalloc is not allowed in a latency-critical loop,

@@ -39,6 +39,8 @@ PDE_BC_FUNC_RAMP = 1
 PDE_FUSED_MAX_COMP = 4
 PDE_MAX_GROUPS = 16
 PDE_NOALLOC_MAX_FLOATS = 1 << 22
+PDE_BATCH_HEAT = 0
+PDE_BATCH_WAVE = 1
 FACE_BITS = {"-X": 1 << 0, "+X": 1 << 1, "-Y": 1 << 2, "+Y": 1 << 3, "-Z": 1 << 4, "+Z": 1 << 5}
 
 
@@ -70,6 +72,18 @@ class PdeBCRules(C.Structure):
 
 class PdeLDCParams(C.Structure):
     _fields_ = [("nu", C.c_float), ("dt", C.c_float), ("jacobi_iters", C.c_int32), ("jacobi_per_pass", C.c_int32)]
+
+
+class PdeBatchGrid(C.Structure):
+    _fields_ = [("field", C.c_void_p), ("field_prev", C.c_void_p), ("scratch", C.c_void_p),
+                ("shape", C.c_int64 * 2), ("dx", C.c_double), ("coef", C.c_float), ("dt", C.c_float)]
+
+
+class PdeBatchPlan(C.Structure):
+    _fields_ = [("table", C.c_void_p), ("kind", C.c_int32), ("ngrids", C.c_int32), ("total_tiles", C.c_int32),
+                ("ghost_cells", C.c_int32), ("order", C.c_int32), ("tile_x", C.c_int32), ("tile_y", C.c_int32),
+                ("steps_per_pass", C.c_int32), ("blocks", C.c_int32), ("smem_bytes", C.c_int32),
+                ("rules", PdeBCRules)]
 
 
 class PdeError(RuntimeError):
@@ -113,6 +127,12 @@ _SIGS = {
                                    C.POINTER(PdeGrid), C.c_void_p]),
     "pde_wave_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(PdeGrid), C.c_void_p]),
+    "pde_batch_work_bytes": (C.c_int, [C.POINTER(PdeBatchGrid), C.c_int32, C.c_int32, C.c_int32,
+                                       C.POINTER(C.c_uint64)]),
+    "pde_batch_plan": (C.c_int, [C.c_int32, C.POINTER(PdeBatchGrid), C.c_int32, C.c_int32, C.c_int32,
+                                 C.POINTER(PdeBCRules), C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_uint64,
+                                 C.POINTER(PdeBatchPlan), C.c_void_p]),
+    "pde_batch_rollout": (C.c_int, [C.POINTER(PdeBatchPlan), C.c_int32, C.c_void_p]),
     "pde_heat_rollout_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                            C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                            C.c_void_p]),

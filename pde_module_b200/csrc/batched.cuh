@@ -1,0 +1,235 @@
+// Batched rollouts: many independent 2D grids of uneven sizes advance nsteps
+// in ONE persistent launch driven by a tile work queue.  The reference advances
+// each grid with its own module chain (examples/2D_Heat_Equation.py:57-65:
+// GridBoundary -> Laplacian -> ForwardEuler, three launches per step).
+//
+// Work items are (time block, grid, tile) triples in time-block-major order,
+// taken from a global counter by persistent blocks.  An item runs the block's
+// steps on its tile grown by a halo H (heat: k*R + 1 as heat2d_tb_kernel; wave:
+// k as wave_fwd_tb_kernel), reading the grid's buffers of the block's parity
+// and writing the others.  Before it starts it waits until the 3x3
+// neighbouring tiles of its grid have finished the previous time block: their
+// output is its input, and they no longer read the buffers it overwrites (the
+// halo is at most one tile wide, so no other tile is involved).  An item only
+// waits on items taken before it, which running blocks hold, so the queue
+// cannot deadlock; every wait is still bounded (~2 s, then PDE_ERR_TIMEOUT is
+// recorded and the block goes on).  A tile publishes its progress with a
+// release store after a __threadfence; waiters read it with acquire loads.
+//
+// Heat step (per grid alpha, dt, dx):  u2 = BC(u);  u = u2 + dt*(alpha*Lap(u2)),
+//   the arithmetic of heat2d_tb_kernel, bit-identical to pde_heat_rollout.
+// Wave step (per grid K = dt^2 c^2):   u^{n+1} = 2u^n - u^{n-1} + K*Lap(u^n) on
+//   the cells inside the node ring, zero elsewhere, as wave_fwd_tb_kernel with
+//   a constant K field and no source.
+#pragma once
+#include "common.cuh"
+#include "fused.cuh"
+#include "tma.cuh"
+
+namespace pde {
+
+enum { BATCH_HEAT = 0, BATCH_WAVE = 1 };
+
+struct BatchGridDev {
+  float* a0;          // parity-0 input: heat u; wave u^n
+  float* a1;          // wave u^{n-1} (parity 0)
+  float* b0;          // parity-1 buffers (scratch)
+  float* b1;
+  int X, Y;           // array extents incl. ghosts (Z = 1, one component)
+  int tiles_y;        // tiles along Y
+  int tile_base;      // first queue index of this grid's tiles
+  int ntiles;
+  float coef, dt, dx32;  // heat: alpha, dt, dx; wave: K
+  float w[5];         // Laplacian weights of this grid's dx
+};
+
+struct BatchParams {
+  const BatchGridDev* grids;
+  int ngrids;
+  int total_tiles;
+  int ntb;            // time blocks (even: the result lands in the parity-0 buffers)
+  int nsteps;         // steps of time block tb: nsteps / ntb + (tb < nsteps % ntb)
+  int H;              // halo of the longest block
+  int TBX, TBY;
+  int RC;             // region capacity (cells)
+  int g;
+  unsigned int* counter;   // work queue head (zeroed before the launch)
+  unsigned int* progress;  // per tile: completed time blocks (zeroed before the launch)
+};
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait until *p >= target.  Returns false on timeout (~2 s).
+__device__ __forceinline__ bool wait_at_least(const unsigned* p, unsigned target) {
+  if (ld_acquire_gpu(p) >= target) return true;
+  const uint64_t t0 = globaltimer_ns();
+  for (uint32_t it = 0;; ++it) {
+    __nanosleep(100);
+    if (ld_acquire_gpu(p) >= target) return true;
+    if ((it & 63u) == 63u && globaltimer_ns() - t0 > 2000000000ull) return false;
+  }
+}
+
+template <int OP, int R>
+__global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const PdeBCRules Rl) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ int s_item;
+  const unsigned total_items = (unsigned)P.total_tiles * (unsigned)P.ntb;
+  const int q = P.nsteps / P.ntb, rmd = P.nsteps % P.ntb;
+  const int H = P.H, g = P.g;
+  bool timed_out = false;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(P.counter, 1u);
+    __syncthreads();
+    const unsigned item = (unsigned)s_item;
+    __syncthreads();  // s_item is rewritten at the top of the next item
+    if (item >= total_items) break;
+    const int tb = (int)(item / (unsigned)P.total_tiles);
+    const int gt = (int)(item - (unsigned)tb * (unsigned)P.total_tiles);
+    int lo = 0, hi = P.ngrids - 1;  // the last grid whose tile_base <= gt
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (P.grids[mid].tile_base <= gt) lo = mid; else hi = mid - 1;
+    }
+    const BatchGridDev& Gd = P.grids[lo];
+    const int X = Gd.X, Y = Gd.Y, tiles_y = Gd.tiles_y;
+    const int lt = gt - Gd.tile_base;
+    const int tx = lt / tiles_y, ty = lt - tx * tiles_y;
+    const int tiles_x = Gd.ntiles / tiles_y;
+    if (tb > 0 && threadIdx.x < 9) {
+      const int nx = tx + (int)threadIdx.x / 3 - 1, ny = ty + (int)threadIdx.x % 3 - 1;
+      if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y && !timed_out) {
+        if (!wait_at_least(P.progress + Gd.tile_base + nx * tiles_y + ny, (unsigned)tb)) {
+          timed_out = true;
+          flag_error(PDE_ERR_TIMEOUT);
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    const int ks = q + (tb < rmd ? 1 : 0);
+    const bool odd = (tb & 1) != 0;
+    const float* in0 = odd ? Gd.b0 : Gd.a0;
+    const float* in1 = odd ? Gd.b1 : Gd.a1;
+    float* out0 = odd ? Gd.a0 : Gd.b0;
+    float* out1 = odd ? Gd.a1 : Gd.b1;
+    const float coef = Gd.coef, dt = Gd.dt, dx32 = Gd.dx32;
+    float w[2 * R + 1];
+#pragma unroll
+    for (int t = 0; t < 2 * R + 1; ++t) w[t] = Gd.w[t];
+    const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
+    const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, X);
+    const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, Y);
+    const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
+    // per-thread walk over the region (flattened, so every lane has a cell):
+    // start at cell tid, advance by blockDim.x = dq rows + dr cells
+    const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
+    const int lx_start = (int)threadIdx.x / RY, ly_start = (int)threadIdx.x - lx_start * RY;
+    float* A;  // buffer holding the newest level after the steps
+    if (OP == BATCH_HEAT) {
+      A = sm;
+      float* B = sm + P.RC;
+      for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+        const int lx = i / RY, ly = i - lx * RY;
+        A[i] = in0[(size_t)(rx0 + lx) * Y + ry0 + ly];
+      }
+      __syncthreads();
+      H2Params HP;
+      HP.X = X; HP.Y = Y; HP.g = g; HP.N = 1;
+      const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
+      const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
+      for (int s = 0; s < ks; ++s) {
+        bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, dx32);
+        int lx = lx_start, ly = ly_start;
+        for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+          const float u2 = A[i];
+          float res = u2;
+          if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(w[t], A[i + (t - R) * RY]));
+#pragma unroll
+            for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(w[t], A[i + (t - R)]));
+            res = add(u2, mul(dt, mul(coef, acc)));
+          }
+          B[i] = res;
+          lx += dq;
+          ly += dr;
+          if (ly >= RY) { ly -= RY; ++lx; }
+        }
+        __syncthreads();
+        float* t = A;
+        A = B;
+        B = t;
+      }
+    } else {
+      float* Bm = sm;
+      float* B0 = sm + P.RC;
+      float* Bp = sm + 2 * P.RC;
+      // the state is zero outside the node ring (x, y in [g+1, n-g-2])
+      for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+        const int lx = i / RY, ly = i - lx * RY;
+        const int x = rx0 + lx, y = ry0 + ly;
+        const bool inside = x > g && x < X - 1 - g && y > g && y < Y - 1 - g;
+        const size_t gi = (size_t)x * Y + y;
+        Bm[i] = inside ? in1[gi] : 0.0f;
+        B0[i] = inside ? in0[gi] : 0.0f;
+      }
+      __syncthreads();
+      for (int s = 0; s < ks; ++s) {
+        int lx = lx_start, ly = ly_start;
+        for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+          const int x = rx0 + lx, y = ry0 + ly;
+          float v = 0.0f;
+          if (x > g && x < X - 1 - g && y > g && y < Y - 1 - g) {
+            if (lx >= 1 && lx < RX - 1 && ly >= 1 && ly < RY - 1) {
+              float acc = 0.0f;  // Laplacian, alpha 1 (FDM/kernel/laplacian.py:40-46 order)
+              acc = add(acc, mul(w[0], B0[i - RY]));
+              acc = add(acc, mul(w[1], B0[i]));
+              acc = add(acc, mul(w[2], B0[i + RY]));
+              acc = add(acc, mul(w[0], B0[i - 1]));
+              acc = add(acc, mul(w[1], B0[i]));
+              acc = add(acc, mul(w[2], B0[i + 1]));
+              v = add(sub(mul(2.0f, B0[i]), Bm[i]), mul(coef, acc));
+            } else {
+              v = B0[i];  // cut edge: not valid after this step, never output
+            }
+          }
+          Bp[i] = v;
+          lx += dq;
+          ly += dr;
+          if (ly >= RY) { ly -= RY; ++lx; }
+        }
+        __syncthreads();
+        float* t = Bm;
+        Bm = B0;
+        B0 = Bp;
+        Bp = t;
+      }
+      A = B0;
+      const int OX = min(bx0 + P.TBX, X) - bx0, OY = min(by0 + P.TBY, Y) - by0;
+      for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
+        const int lx = i / OY, ly = i - lx * OY;
+        out1[(size_t)(bx0 + lx) * Y + by0 + ly] = Bm[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+      }
+    }
+    const int OX = min(bx0 + P.TBX, X) - bx0, OY = min(by0 + P.TBY, Y) - by0;
+    for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
+      const int lx = i / OY, ly = i - lx * OY;
+      out0[(size_t)(bx0 + lx) * Y + by0 + ly] = A[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release_gpu(P.progress + gt, (unsigned)(tb + 1));
+  }
+}
+
+}  // namespace pde

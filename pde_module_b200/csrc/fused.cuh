@@ -23,11 +23,15 @@ __device__ __forceinline__ int node_class_axis(int64_t i, int64_t n, int g, bool
 
 // Value written into a ghost component by group `gi` from the pre-boundary
 // neighbour value `a` (inc = +1 for a low-side node, -1 for a high-side node).
-__device__ __forceinline__ float ghost_value(const PdeBCRules& Rl, int gi, int inc, float a) {
+__device__ __forceinline__ float ghost_value(const PdeBCRules& Rl, int gi, int inc, float a, float dx32) {
   const PdeBCGroupParam& G = Rl.group[gi];
   const float v = G.value;  // constant groups only on fused paths
   if (G.type == PDE_BC_DIRICHLET) return sub(mul(2.0f, v), a);
-  return add(mul(mul((float)(-2 * inc), Rl.dx32), v), a);
+  return add(mul(mul((float)(-2 * inc), dx32), v), a);
+}
+
+__device__ __forceinline__ float ghost_value(const PdeBCRules& Rl, int gi, int inc, float a) {
+  return ghost_value(Rl, gi, inc, a, Rl.dx32);
 }
 
 // Boundary-filled value u2 at cell (c0,c1,c2), component v, of the field
@@ -141,7 +145,7 @@ struct H2Params {
 // in place: ghosts first (they read pre-boundary interior values), then nodes.
 template <int N>
 __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, const PdeBCRules& Rl, int rx0, int RX,
-                                               int ry0, int RY) {
+                                               int ry0, int RY, float dx32) {
   const int g = P.g, X = P.X, Y = P.Y;
   const int nthr = blockDim.x, tid = threadIdx.x;
   // ghost strips: x = g-1 (low), x = X-g (high), partner rows y in [g, Y-g)
@@ -175,7 +179,7 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
       const int gi = Rl.ghost_group[K][ax][v];
       if (gi < 0) continue;
       const float a = A[((qx - rx0) * RY + (qy - ry0)) * N + v];
-      A[((gx - rx0) * RY + (gy - ry0)) * N + v] = ghost_value(Rl, gi, inc, a);
+      A[((gx - rx0) * RY + (gy - ry0)) * N + v] = ghost_value(Rl, gi, inc, a, dx32);
     }
   }
   __syncthreads();
@@ -234,7 +238,7 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
   const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(P.X - g, rx0 + RX - R) - rx0;
   const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(P.Y - g, ry0 + RY - R) - ry0;
   for (int s = 0; s < P.k; ++s) {
-    bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY);
+    bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
     for (int lx = lx0; lx < RX; lx += nrows)
       for (int lf = lf0; lf < nrow; lf += 32) {
         const int idx = lx * nrow + lf;

@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restric
   const int sy0 = max(g, ry0 + 1) - ry0, sy1 = min(P.Y - g, ry0 + RY - 1) - ry0;
   float sq = 0.0f;
   for (int s = 0; s < P.k; ++s) {
-    bc_fill_region<1>(A, HP, Rp, rx0, RX, ry0, RY);
+    bc_fill_region<1>(A, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);
     const bool acc_res = P.last && s == P.k - 1;
     for (int lx = lx0; lx < RX; lx += nrows)
       for (int ly = ly0; ly < RY; ly += 32) {

@@ -10,6 +10,7 @@
 #include "fused.cuh"
 #include "ldc.cuh"
 #include "wave.cuh"
+#include "batched.cuh"
 
 using namespace pde;
 
@@ -718,6 +719,180 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
     if (rc) return rc;
   }
   return PDE_OK;
+}
+
+}  // extern "C"
+
+// ---- batched rollouts --------------------------------------------------------
+namespace {
+
+constexpr int BATCH_TILE_X = 32, BATCH_TILE_Y = 64, BATCH_K = 8;
+constexpr size_t BATCH_QUEUE_OFF_ALIGN = 256;
+
+size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// work layout: [descriptor table][queue counter, 256 B][progress: u32 per tile]
+bool batch_layout(const PdeBatchGrid* grids, int ngrids, int tx, int ty, int64_t* total_tiles, size_t* table_bytes,
+                  size_t* bytes) {
+  int64_t tiles = 0;
+  for (int i = 0; i < ngrids; ++i) {
+    const int64_t X = grids[i].shape[0], Y = grids[i].shape[1];
+    if (X < 1 || Y < 1 || X > (1 << 30) || Y > (1 << 30)) return false;
+    tiles += ((X + tx - 1) / tx) * ((Y + ty - 1) / ty);
+  }
+  if (tiles <= 0 || tiles > (1LL << 30)) return false;
+  *total_tiles = tiles;
+  *table_bytes = round_up((size_t)ngrids * sizeof(BatchGridDev), BATCH_QUEUE_OFF_ALIGN);
+  *bytes = *table_bytes + BATCH_QUEUE_OFF_ALIGN + (size_t)tiles * sizeof(unsigned);
+  return true;
+}
+
+int batch_halo(int kind, int order, int k) { return kind == PDE_BATCH_HEAT ? k * (order / 2) + 1 : k; }
+
+template <int OP, int R>
+int batch_occupancy(int smem, int* occ) {
+  auto kern = batched_kernel<OP, R>;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  int o = 0;
+  PDE_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 256, smem));
+  if (o < 1) return PDE_ERR_TOO_LARGE;
+  *occ = o;
+  return PDE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pde_batch_work_bytes(const PdeBatchGrid* grids, int32_t ngrids, int32_t tile_x, int32_t tile_y,
+                         uint64_t* bytes) {
+  if (!grids || ngrids < 1 || !bytes || tile_x < 0 || tile_y < 0) return PDE_ERR_ARG;
+  const int tx = tile_x > 0 ? tile_x : BATCH_TILE_X, ty = tile_y > 0 ? tile_y : BATCH_TILE_Y;
+  int64_t tiles;
+  size_t tb, b;
+  if (!batch_layout(grids, ngrids, tx, ty, &tiles, &tb, &b)) return PDE_ERR_SHAPE;
+  *bytes = b;
+  return PDE_OK;
+}
+
+int pde_batch_plan(int32_t kind, const PdeBatchGrid* grids, int32_t ngrids, int32_t ghost_cells, int32_t order,
+                   const PdeBCRules* rules, int32_t tile_x, int32_t tile_y, int32_t steps_per_pass, void* work,
+                   uint64_t work_bytes, PdeBatchPlan* plan, void* stream) {
+  if (!grids || ngrids < 1 || !work || !plan || tile_x < 0 || tile_y < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
+  if (kind != PDE_BATCH_HEAT && kind != PDE_BATCH_WAVE) return PDE_ERR_ARG;
+  if (order != 2 && order != 4) return PDE_ERR_ARG;
+  if (kind == PDE_BATCH_WAVE && order != 2) return PDE_ERR_UNSUPPORTED;
+  if (ghost_cells < order / 2 || ghost_cells < 1) return PDE_ERR_GHOST;
+  if (kind == PDE_BATCH_HEAT) {
+    if (!rules) return PDE_ERR_ARG;
+    if (rules->ncomp != 1) return PDE_ERR_ARG;
+    if (rules->has_ramp) return PDE_ERR_UNSUPPORTED;
+  }
+  if ((reinterpret_cast<uintptr_t>(work) & (BATCH_QUEUE_OFF_ALIGN - 1)) != 0) return PDE_ERR_ALIGN;
+  const int tx = tile_x > 0 ? tile_x : BATCH_TILE_X, ty = tile_y > 0 ? tile_y : BATCH_TILE_Y;
+  const int k = steps_per_pass > 0 ? steps_per_pass : BATCH_K;
+  const int H = batch_halo(kind, order, k);
+  if (H > tx || H > ty || tx > 4096 || ty > 4096) return PDE_ERR_ARG;
+  int64_t tiles;
+  size_t table_bytes, bytes;
+  if (!batch_layout(grids, ngrids, tx, ty, &tiles, &table_bytes, &bytes)) return PDE_ERR_SHAPE;
+  if (work_bytes < bytes) return PDE_ERR_TOO_LARGE;
+  const int nbuf = kind == PDE_BATCH_HEAT ? 2 : 3;
+  const size_t smem = (size_t)nbuf * (tx + 2 * H) * (ty + 2 * H) * sizeof(float);
+  if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  BatchGridDev* host = new BatchGridDev[ngrids];
+  int64_t base = 0;
+  for (int i = 0; i < ngrids; ++i) {
+    const PdeBatchGrid& B = grids[i];
+    const int64_t X = B.shape[0], Y = B.shape[1];
+    const bool ok = B.field && B.scratch && (kind == PDE_BATCH_HEAT || B.field_prev) && B.dx > 0.0 &&
+                    X > 2 * ghost_cells + 1 && Y > 2 * ghost_cells + 1 && B.field != B.scratch &&
+                    B.field_prev != B.field;
+    if (!ok) {
+      delete[] host;
+      return X > 2 * ghost_cells + 1 && Y > 2 * ghost_cells + 1 ? PDE_ERR_ARG : PDE_ERR_SHAPE;
+    }
+    BatchGridDev& D = host[i];
+    memset(&D, 0, sizeof(D));
+    const size_t cells = (size_t)X * Y;
+    D.a0 = B.field;
+    D.a1 = kind == PDE_BATCH_WAVE ? B.field_prev : nullptr;
+    D.b0 = B.scratch;
+    D.b1 = kind == PDE_BATCH_WAVE ? B.scratch + cells : nullptr;
+    D.X = (int)X;
+    D.Y = (int)Y;
+    D.tiles_y = (int)((Y + ty - 1) / ty);
+    D.ntiles = (int)(((X + tx - 1) / tx) * D.tiles_y);
+    D.tile_base = (int)base;
+    base += D.ntiles;
+    D.coef = B.coef;
+    D.dt = B.dt;
+    D.dx32 = (float)B.dx;
+    const Weights W = lap_weights(order, B.dx);
+    for (int t = 0; t < 5; ++t) D.w[t] = W.w[t];
+  }
+  cudaStream_t st = as_stream(stream);
+  const cudaError_t ce = cudaMemcpyAsync(work, host, (size_t)ngrids * sizeof(BatchGridDev), cudaMemcpyHostToDevice, st);
+  delete[] host;
+  if (ce != cudaSuccess) return PDE_ERR_CUDA;
+  int occ = 0, rc;
+  if (kind == PDE_BATCH_HEAT)
+    rc = order == 2 ? batch_occupancy<BATCH_HEAT, 1>((int)smem, &occ) : batch_occupancy<BATCH_HEAT, 2>((int)smem, &occ);
+  else
+    rc = batch_occupancy<BATCH_WAVE, 1>((int)smem, &occ);
+  if (rc) return rc;
+  memset(plan, 0, sizeof(*plan));
+  plan->table = work;
+  plan->kind = kind;
+  plan->ngrids = ngrids;
+  plan->total_tiles = (int32_t)tiles;
+  plan->ghost_cells = ghost_cells;
+  plan->order = order;
+  plan->tile_x = tx;
+  plan->tile_y = ty;
+  plan->steps_per_pass = k;
+  plan->blocks = occ * sm_count();
+  plan->smem_bytes = (int32_t)smem;
+  if (kind == PDE_BATCH_HEAT) plan->rules = *rules;
+  return PDE_OK;
+}
+
+int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream) {
+  if (!plan || !plan->table || nsteps < 0 || plan->steps_per_pass < 1 || plan->total_tiles < 1) return PDE_ERR_ARG;
+  if (nsteps == 0) return PDE_OK;
+  const int k = plan->steps_per_pass;
+  int ntb = (nsteps + k - 1) / k;
+  ntb += ntb & 1;  // even: the last block writes the parity-0 buffers (the caller's fields)
+  if ((int64_t)ntb * plan->total_tiles >= (1LL << 31) - (int64_t)plan->blocks) return PDE_ERR_TOO_LARGE;
+  const int kmax = (nsteps + ntb - 1) / ntb;
+  size_t table_bytes = round_up((size_t)plan->ngrids * sizeof(BatchGridDev), BATCH_QUEUE_OFF_ALIGN);
+  char* base = static_cast<char*>(plan->table);
+  BatchParams P;
+  P.grids = reinterpret_cast<const BatchGridDev*>(base);
+  P.ngrids = plan->ngrids;
+  P.total_tiles = plan->total_tiles;
+  P.ntb = ntb;
+  P.nsteps = nsteps;
+  P.H = batch_halo(plan->kind, plan->order, kmax);
+  P.TBX = plan->tile_x;
+  P.TBY = plan->tile_y;
+  const int Hp = batch_halo(plan->kind, plan->order, k);
+  P.RC = (plan->tile_x + 2 * Hp) * (plan->tile_y + 2 * Hp);
+  P.g = plan->ghost_cells;
+  P.counter = reinterpret_cast<unsigned*>(base + table_bytes);
+  P.progress = reinterpret_cast<unsigned*>(base + table_bytes + BATCH_QUEUE_OFF_ALIGN);
+  cudaStream_t st = as_stream(stream);
+  PDE_CUDA_CHECK(cudaMemsetAsync(P.counter, 0, BATCH_QUEUE_OFF_ALIGN + (size_t)plan->total_tiles * sizeof(unsigned), st));
+  const int64_t items = (int64_t)ntb * plan->total_tiles;
+  const int blocks = (int)(items < plan->blocks ? items : plan->blocks);
+  const size_t smem = (size_t)plan->smem_bytes;
+  if (plan->kind == PDE_BATCH_HEAT) {
+    if (plan->order == 2) batched_kernel<BATCH_HEAT, 1><<<blocks, 256, smem, st>>>(P, plan->rules);
+    else batched_kernel<BATCH_HEAT, 2><<<blocks, 256, smem, st>>>(P, plan->rules);
+  } else {
+    batched_kernel<BATCH_WAVE, 1><<<blocks, 256, smem, st>>>(P, plan->rules);
+  }
+  return launch_status();
 }
 
 }  // extern "C"

@@ -79,3 +79,39 @@ def tune_heat_depth(rollout, u: torch.Tensor, nsteps: int = 256, depths=(1, 2, 4
             best, best_ms = k, ms
     rollout.steps_per_pass = best
     return best
+
+
+BATCH_TILES = ((32, 64), (64, 64), (32, 128), (64, 32), (16, 128), (48, 96))
+BATCH_DEPTHS = (2, 4, 6, 8, 12, 16)
+
+
+def tune_batched(rollout, nsteps: int = 100, tiles=BATCH_TILES, depths=BATCH_DEPTHS, reps: int = 2) -> dict:
+    """Pick the fastest (tile, time-block depth) of a batched rollout.
+
+    Times ``rollout(nsteps)`` for every admissible pair (the halo may not exceed
+    a tile side, the shared-memory region must fit) and leaves the rollout
+    configured with the best.  The rollout advances its fields in place, so
+    they are saved first and restored afterwards.  Returns
+    {"best": (tile_x, tile_y, k), "ms": {"TXxTY_k": ms}}."""
+    saved = [f.clone() for f in rollout.fields]
+    saved_prev = [f.clone() for f in rollout.prev] if rollout.prev is not None else None
+    times = {}
+    best = None
+    for t in tiles:
+        for k in depths:
+            try:
+                rollout.configure(tile=t, steps_per_pass=k)
+            except _lib.PdeError:
+                continue  # halo wider than the tile, or region too large
+            ms = _time(lambda: rollout(nsteps), reps)
+            times[f"{t[0]}x{t[1]}_k{k}"] = round(ms, 4)
+            if best is None or ms < best[0]:
+                best = (ms, t, k)
+    rollout.configure(tile=best[1], steps_per_pass=best[2])
+    for f, s in zip(rollout.fields, saved):
+        f.copy_(s)
+    if saved_prev is not None:
+        for f, s in zip(rollout.prev, saved_prev):
+            f.copy_(s)
+    torch.cuda.synchronize()
+    return {"best": (best[1][0], best[1][1], best[2]), "ms": times}

@@ -139,3 +139,59 @@ def test_compiled_rules_match_group_semantics(shape, g, N, spec):
     r = compile_rules(shape, g, N, spec, dx)
     got = apply_rules(u, r, g, dx)
     np.testing.assert_array_equal(got, ref)
+
+
+def _batch_desc(shapes, ptr0=1 << 20):
+    arr = (_lib.PdeBatchGrid * len(shapes))()
+    for i, (X, Y) in enumerate(shapes):
+        arr[i].field = ptr0 + i * (1 << 16)
+        arr[i].field_prev = ptr0 + (1 << 30) + i * (1 << 16)
+        arr[i].scratch = ptr0 + (1 << 31) + i * (1 << 16)
+        arr[i].shape[0], arr[i].shape[1] = X, Y
+        arr[i].dx, arr[i].coef, arr[i].dt = 0.1, 1.0, 0.001
+    return arr
+
+
+def test_batch_plan_validation_needs_no_gpu():
+    L = _lib.lib()
+    shapes = [(66, 130), (10, 7), (1026, 514)]
+    desc = _batch_desc(shapes)
+    nb = C.c_uint64(0)
+    assert L.pde_batch_work_bytes(desc, 3, 32, 64, C.byref(nb)) == _lib.PDE_OK
+    tiles = sum(-(-X // 32) * -(-Y // 64) for X, Y in shapes)
+    # descriptor table (device layout, 256-byte aligned) + queue head + one progress word per tile
+    assert 4 * tiles + 512 <= nb.value <= 4 * tiles + 256 + 256 * 3
+    assert L.pde_batch_work_bytes(desc, 0, 32, 64, C.byref(nb)) == _lib.PDE_ERR_ARG
+    bad = _batch_desc([(0, 10)])
+    assert L.pde_batch_work_bytes(bad, 1, 32, 64, C.byref(nb)) == _lib.PDE_ERR_SHAPE
+    # rules for the heat kind: Dirichlet 0 on every face of a 2D grid
+    grp = (_lib.PdeBCGroup * 1)()
+    grp[0].type, grp[0].comp_mask, grp[0].face_mask = _lib.PDE_BC_DIRICHLET, 1, 0xF
+    rules = _lib.PdeBCRules()
+    g2 = _lib.make_grid((66, 130, 1), 1, 2, 0.1)
+    assert L.pde_bc_compile(grp, 1, C.byref(g2), 1, C.byref(rules)) == _lib.PDE_OK
+    plan = _lib.PdeBatchPlan()
+    work = C.c_void_p(1 << 24)
+    big = 1 << 30
+
+    def plan_rc(kind=_lib.PDE_BATCH_HEAT, d=desc, n=3, g=1, order=2, r=rules, tx=32, ty=64, k=8, w=work, wb=big):
+        return L.pde_batch_plan(kind, d, n, g, order, C.byref(r) if r is not None else None, tx, ty, k, w, wb,
+                                C.byref(plan), None)
+
+    assert plan_rc(kind=7) == _lib.PDE_ERR_ARG
+    assert plan_rc(order=3) == _lib.PDE_ERR_ARG
+    assert plan_rc(kind=_lib.PDE_BATCH_WAVE, order=4, g=2) == _lib.PDE_ERR_UNSUPPORTED
+    assert plan_rc(g=0) == _lib.PDE_ERR_GHOST
+    assert plan_rc(r=None) == _lib.PDE_ERR_ARG
+    assert plan_rc(k=40) == _lib.PDE_ERR_ARG        # halo 41 wider than the 32-cell tile side
+    assert plan_rc(tx=16, k=16) == _lib.PDE_ERR_ARG
+    assert plan_rc(wb=16) == _lib.PDE_ERR_TOO_LARGE
+    assert plan_rc(w=C.c_void_p((1 << 24) + 4)) == _lib.PDE_ERR_ALIGN
+    assert plan_rc(tx=256, ty=256, k=16) == _lib.PDE_ERR_TOO_LARGE  # shared-memory region too large
+    tiny = _batch_desc([(3, 40)])
+    assert plan_rc(d=tiny, n=1) == _lib.PDE_ERR_SHAPE
+    ramp = _lib.PdeBCRules.from_buffer_copy(rules)
+    ramp.has_ramp = 1
+    assert plan_rc(r=ramp) == _lib.PDE_ERR_UNSUPPORTED
+    assert L.pde_batch_rollout(None, 5, None) == _lib.PDE_ERR_ARG
+    assert L.pde_batch_rollout(C.byref(_lib.PdeBatchPlan()), 5, None) == _lib.PDE_ERR_ARG
