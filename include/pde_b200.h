@@ -223,6 +223,24 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
                      int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
                      int32_t nsteps, int32_t steps_per_pass, void* stream);
 
+/* ---- differentiable heat rollout (new: the reference has the forward loop
+ * only, examples/2D_Heat_Equation.py:57-65, with a scalar alpha) ----
+ * 2D grids, one component, order 2 or 4, constant-valued face groups.
+ * Forward step with a per-cell diffusivity field alpha (X, Y):
+ *   v = BC(u);  S = Lap(v) (alpha 1);  u' = v + dt*(alpha o S) on stencil cells, v elsewhere
+ * (bit-identical to pde_heat_rollout when alpha is constant).  `lstates`, if
+ * not NULL, receives S of step n at lstates + n*X*Y for n = 0..nsteps-1 (0
+ * off the stencil cells).  `work`: one field of scratch. */
+int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                     const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
+                     void* stream);
+/* Discrete adjoint of nsteps forward steps: lam_in = dJ/du^N, lam_out =
+ * dJ/du^0; grad_alpha += dJ/dalpha (accumulated in step order n = N-1..0);
+ * lstates as written by pde_heat_forward for the same steps. */
+int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, const float* lstates,
+                     float* grad_alpha, const PdeGrid* grid, const PdeBCRules* rules, float dt, int32_t nsteps,
+                     int32_t steps_per_pass, float* work, void* stream);
+
 /* ---- fractional-step lid-driven cavity (new: the reference's LDC uses
  * artificial compressibility, examples/LDC/LDC_Graph_Capture.py:71-90) ---- */
 typedef struct PdeLDCParams {

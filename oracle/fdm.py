@@ -264,6 +264,88 @@ def heat_rollout(u: np.ndarray, groups: list, dx: float, ghost: int, alpha: floa
     return u
 
 
+def heat_forward_field(alpha, u0, groups, dx, ghost, dt, nsteps, order=2, dtype=np.float32):
+    """New (the reference's loop, examples/2D_Heat_Equation.py:57-65, has a scalar
+    alpha): the heat step with a per-cell diffusivity field, one component,
+        v = B(u);  S = L(v) (alpha 1);  u' = v + dt*(alpha o S).
+    alpha, u0: (X, Y, Z, 1).  Returns (u^N, [S^0, ..., S^{N-1}]), S as (X, Y, Z) arrays."""
+    u = np.asarray(u0, dtype=dtype)
+    a = np.asarray(alpha, dtype=dtype)
+    S = []
+    for _ in range(nsteps):
+        v = bc_apply(u, groups, dx, ghost, dtype=dtype)
+        acc = laplacian(v, dx, ghost, 1.0, order, dtype)
+        S.append(acc[..., 0].copy())
+        u = forward_euler(v, a * acc, dt, dtype)
+    return u, S
+
+
+def bc_linear_map(grid_shape, groups, dx, ghost):
+    """The linear part of the boundary fill B(u) = A u + b (one component):
+    (direct, pairs) with direct[i] true where B(u)_i = u_i, and pairs a list of
+    (ghost cell, partner cell, coefficient +-1) for B(u)_ghost = c +- u_partner.
+    Found by applying bc_apply to cell ids with every value set to 0."""
+    n = int(np.prod(grid_shape[:3]))
+    ids = (np.arange(n, dtype=np.float64) + 1.0).reshape(tuple(grid_shape[:3]) + (1,))
+    zero = [dict(G, value=0.0) for G in groups]
+    out = bc_apply(ids, zero, dx, ghost, dtype=np.float64).reshape(-1)
+    flat = ids.reshape(-1)
+    direct = out == flat
+    pairs = []
+    for i in np.nonzero((out != flat) & (out != 0.0))[0]:
+        p = int(abs(out[i])) - 1
+        pairs.append((int(i), p, 1.0 if out[i] > 0 else -1.0))
+    return direct.reshape(grid_shape[:3]), pairs
+
+
+def heat_adjoint(alpha, S, lamN, groups, dx, ghost, dt, order=2, dtype=np.float32):
+    """Discrete adjoint of heat_forward_field, one rounding per operation:
+        dJ/dalpha += lam o (dt * S^n)          stencil cells, n = N-1 .. 0
+        z  = dt * (alpha o lam)                stencil cells, 0 elsewhere
+        mu = lam + L^T(z)                      L^T = L, zero outside the array
+        lam = B^T(mu): (direct ? mu : 0), then -/+ mu_ghost per pair, ghosts in
+              the order x-low, x-high, y-low, y-high of their partner.
+    Returns (dJ/dalpha, dJ/du^0) as (X, Y, Z, 1) arrays."""
+    a = np.asarray(alpha, dtype=dtype)[..., 0]
+    lam = np.array(np.asarray(lamN, dtype=dtype)[..., 0])
+    gs = lam.shape
+    direct, pairs = bc_linear_map(gs, groups, dx, ghost)
+    strides = (gs[1] * gs[2], gs[2], 1)
+
+    def pair_key(pr):
+        gcell, pcell, _ = pr
+        d = pcell - gcell
+        axis = next(ax for ax in range(3) if strides[ax] == abs(d) // 2 and abs(d) % strides[ax] == 0)
+        return (pcell, axis, 0 if d > 0 else 1)  # per partner: axis, then the low-side ghost first
+
+    pairs = sorted(pairs, key=pair_key)
+    w = lap_weights(order, dx, dtype)
+    R = (len(w) - 1) // 2
+    core = _interior_slices(gs, ghost)
+    st = np.zeros(gs, dtype=bool)
+    st[core] = True
+    galpha = np.zeros(gs, dtype=dtype)
+    dt32 = dtype(dt)
+    for n in range(len(S) - 1, -1, -1):
+        galpha[st] = galpha[st] + lam[st] * (dt32 * np.asarray(S[n], dtype=dtype)[st])
+        z = np.zeros(gs, dtype=dtype)
+        z[st] = dt32 * (a[st] * lam[st])
+        zp = np.pad(z, [(R, R) if gs[ax] > 1 else (0, 0) for ax in range(3)])
+        acc = np.zeros(gs, dtype=dtype)
+        for ax in eligible_dims(gs):
+            for t in range(len(w)):
+                sl = [slice(R, R + gs[b]) if gs[b] > 1 else slice(None) for b in range(3)]
+                sl[ax] = slice(t, t + gs[ax])
+                acc = acc + w[t] * zp[tuple(sl)]
+        mu = lam + acc
+        new = np.where(direct, mu, dtype(0)).reshape(-1)
+        muf = mu.reshape(-1)
+        for gcell, pcell, c in pairs:
+            new[pcell] = new[pcell] + muf[gcell] if c > 0 else new[pcell] - muf[gcell]
+        lam = new.reshape(gs)
+    return galpha[..., None], lam[..., None]
+
+
 def standard_groups(grid_shape, ghost, spec) -> list:
     """spec: list of (group_name, type, value, comps) -> group dicts with ids."""
     G = exterior_groups(grid_shape, ghost)

@@ -6,10 +6,11 @@ of include/pde_b200.h in ``_native/libpde_b200.so``.
 """
 from . import _lib
 from .FDM import Laplacian, Grad, Divergence, GridBoundary
-from .time_step import (ForwardEuler, HeatRollout, FractionalStepLDC, WaveSolver, wave_rollout,
+from .time_step import (ForwardEuler, HeatRollout, HeatSolver, heat_rollout, FractionalStepLDC, WaveSolver,
+                        wave_rollout,
                         BatchedHeatRollout, BatchedWaveRollout)
 from .mesh import UniformGridMesh, create_structured_field, create_structured_warp_field
 
 __all__ = ["Laplacian", "Grad", "Divergence", "GridBoundary", "ForwardEuler", "HeatRollout", "FractionalStepLDC",
-           "WaveSolver", "wave_rollout", "BatchedHeatRollout", "BatchedWaveRollout",
+           "HeatSolver", "heat_rollout", "WaveSolver", "wave_rollout", "BatchedHeatRollout", "BatchedWaveRollout",
            "UniformGridMesh", "create_structured_field", "create_structured_warp_field"]

@@ -127,6 +127,12 @@ _SIGS = {
                                    C.POINTER(PdeGrid), C.c_void_p]),
     "pde_wave_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(PdeGrid), C.c_void_p]),
+    "pde_heat_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid),
+                                   C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32, C.c_void_p,
+                                   C.c_void_p]),
+    "pde_heat_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32,
+                                   C.c_void_p, C.c_void_p]),
     "pde_batch_work_bytes": (C.c_int, [C.POINTER(PdeBatchGrid), C.c_int32, C.c_int32, C.c_int32,
                                        C.POINTER(C.c_uint64)]),
     "pde_batch_plan": (C.c_int, [C.c_int32, C.POINTER(PdeBatchGrid), C.c_int32, C.c_int32, C.c_int32,

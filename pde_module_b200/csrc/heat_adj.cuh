@@ -1,0 +1,242 @@
+// Differentiable 2D heat rollout: forward with a per-cell diffusivity field and
+// its discrete adjoint.  New: the reference has the forward loop only
+// (examples/2D_Heat_Equation.py:57-65, scalar alpha).
+//
+// Forward step (scalar field, one component), as heat2d_tb_kernel with alpha
+// taken per cell:
+//   v = B(u^n)                          boundary fill (GridBoundary semantics)
+//   S^n = L(v)   on stencil cells       the reference's Laplacian sum, alpha 1
+//   u^{n+1} = v + dt * (alpha o S^n)    stencil cells;  v elsewhere
+// With a constant field the result is bit-identical to pde_heat_rollout.
+//
+// Adjoint of one step, lam = dJ/du^{n+1} -> dJ/du^n (every product and sum
+// rounded on its own, in the order written):
+//   dJ/dalpha_c += lam_c * (dt * S^n_c)           stencil cells, n = N-1 .. 0
+//   z   = dt * (alpha o lam)                      stencil cells, 0 elsewhere
+//   mu  = lam + L^T(z)                            L^T = L (symmetric weights),
+//                                                 neighbours outside the array 0
+//   lam = B^T(mu):  (cell overwritten by B ? 0 : mu_j)
+//                   then -/+ mu_G for each filled ghost G whose partner is j
+//                   (Dirichlet ghost = 2 val - u_j: -1; Neumann = c + u_j: +1),
+//                   in the order x-low, x-high, y-low, y-high ghost.
+// A ghost's partner is two cells inward (the cell across its node).
+//
+// Temporal blocking as in heat2d_tb_kernel: k steps per pass on shared-memory
+// regions (tile + halo).  Adjoint halo: k*R; cut edges move R cells per step;
+// a region edge that would fall within g+2 cells of the array edge is moved to
+// the array edge, so no ghost/partner pair straddles a cut.
+#pragma once
+#include "common.cuh"
+#include "fused.cuh"
+
+namespace pde {
+
+struct HAParams {
+  int X, Y, g;
+  int k;               // steps in this pass
+  int TBX, TBY, tiles_y;
+  int RC;              // region capacity (cells)
+  float w[5];
+  float dt;
+  long long cells;     // X*Y
+  const float* alpha;  // per-cell diffusivity (X, Y)
+  float* lst;          // forward: if set, S^{n0+s} stored at lst + s*cells
+  const float* lsts;   // adjoint: S^n at lsts + n*cells
+  int ntop;            // adjoint: this pass runs n = ntop, ntop-1, ..., ntop-k+1
+  float* galpha;       // adjoint: dJ/dalpha, accumulated in place
+};
+
+__device__ __forceinline__ bool heat_stencil_cell(int x, int y, int X, int Y, int g) {
+  return x >= g && x < X - g && y >= g && y < Y - g;
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) heat2d_field_fwd_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                                const HAParams P, const PdeBCRules Rl) {
+  extern __shared__ __align__(16) float sm[];
+  const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
+  const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
+  const int H = P.k * R + 1;
+  const int X = P.X, Y = P.Y, g = P.g;
+  const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, X);
+  const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, Y);
+  const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
+  float* A = sm;
+  float* B = sm + P.RC;
+  float* AL = sm + 2 * P.RC;
+  for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+    const int lx = i / RY, ly = i - lx * RY;
+    const size_t gi = (size_t)(rx0 + lx) * Y + ry0 + ly;
+    A[i] = __ldg(in + gi);
+    AL[i] = __ldg(P.alpha + gi);
+  }
+  __syncthreads();
+  H2Params HP;
+  HP.X = X; HP.Y = Y; HP.g = g; HP.N = 1;
+  const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
+  const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
+  const int ox1 = min(bx0 + P.TBX, X), oy1 = min(by0 + P.TBY, Y);
+  const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
+  for (int s = 0; s < P.k; ++s) {
+    bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    float* Ls = P.lst ? P.lst + (size_t)s * P.cells : nullptr;
+    int lx = (int)threadIdx.x / RY, ly = (int)threadIdx.x - lx * RY;
+    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+      const float u2 = A[i];
+      float res = u2, acc = 0.0f;
+      if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
+#pragma unroll
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[i + (t - R) * RY]));
+#pragma unroll
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[i + (t - R)]));
+        res = add(u2, mul(P.dt, mul(AL[i], acc)));
+      }
+      B[i] = res;
+      const int x = rx0 + lx, y = ry0 + ly;
+      if (Ls && x >= bx0 && x < ox1 && y >= by0 && y < oy1) Ls[(size_t)x * Y + y] = acc;
+      lx += dq;
+      ly += dr;
+      if (ly >= RY) { ly -= RY; ++lx; }
+    }
+    __syncthreads();
+    float* t = A;
+    A = B;
+    B = t;
+  }
+  const int OX = ox1 - bx0, OY = oy1 - by0;
+  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
+    const int lx = i / OY, ly = i - lx * OY;
+    out[(size_t)(bx0 + lx) * Y + by0 + ly] = A[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+  }
+}
+
+// Is cell (x, y) overwritten by the boundary fill (a filled ghost or a
+// Dirichlet node)?  2D, one component.
+__device__ __forceinline__ bool bc_overwritten(const PdeBCRules& Rl, int x, int y, int X, int Y, int g) {
+  const bool yin = y >= g && y < Y - g, xin = x >= g && x < X - g;
+  if (yin && (x == g - 1 || x == X - g)) {
+    const int px = x == g - 1 ? g : X - g - 1;
+    const int K = node_class_axis(px, X, g, true) * 9 + node_class_axis(y, Y, g, true) * 3 + 1;
+    return Rl.ghost_group[K][0][0] >= 0;
+  }
+  if (xin && (y == g - 1 || y == Y - g)) {
+    const int py = y == g - 1 ? g : Y - g - 1;
+    const int K = node_class_axis(x, X, g, true) * 9 + node_class_axis(py, Y, g, true) * 3 + 1;
+    return Rl.ghost_group[K][1][0] >= 0;
+  }
+  if (xin && yin && (x == g || x == X - g - 1 || y == g || y == Y - g - 1)) {
+    const int K = node_class_axis(x, X, g, true) * 9 + node_class_axis(y, Y, g, true) * 3 + 1;
+    const int gi = Rl.node_group[K];
+    return gi >= 0 && (Rl.group[gi].comp_mask & 1u);
+  }
+  return false;
+}
+
+// mu of the ghost across node (px, py) on `axis`, folded into v with its sign.
+__device__ __forceinline__ float bt_ghost(const PdeBCRules& Rl, float v, float mG, int px, int py, int axis, int X,
+                                          int Y, int g) {
+  const int K = node_class_axis(px, X, g, true) * 9 + node_class_axis(py, Y, g, true) * 3 + 1;
+  const int gi = Rl.ghost_group[K][axis][0];
+  if (gi < 0) return v;
+  return Rl.group[gi].type == PDE_BC_DIRICHLET ? sub(v, mG) : add(v, mG);
+}
+
+template <int R>
+__global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict__ lam_in,
+                                                          float* __restrict__ lam_out, const HAParams P,
+                                                          const PdeBCRules Rl) {
+  extern __shared__ __align__(16) float sm[];
+  const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
+  const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
+  const int H = P.k * R;
+  const int X = P.X, Y = P.Y, g = P.g;
+  int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, X);
+  int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, Y);
+  if (rx0 <= g + 1) rx0 = 0;
+  if (rx1 >= X - g - 1) rx1 = X;
+  if (ry0 <= g + 1) ry0 = 0;
+  if (ry1 >= Y - g - 1) ry1 = Y;
+  const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
+  const int ox1 = min(bx0 + P.TBX, X), oy1 = min(by0 + P.TBY, Y);
+  const int OX = ox1 - bx0, OY = oy1 - by0;
+  float* Lm = sm;
+  float* Z = sm + P.RC;
+  float* M = sm + 2 * P.RC;
+  float* AL = sm + 3 * P.RC;
+  float* GA = sm + 4 * P.RC;  // dJ/dalpha of the tile (OX x OY)
+  const float dt = P.dt;
+  for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+    const int lx = i / RY, ly = i - lx * RY;
+    const int x = rx0 + lx, y = ry0 + ly;
+    const size_t gi = (size_t)x * Y + y;
+    const float l = __ldg(lam_in + gi), a = __ldg(P.alpha + gi);
+    Lm[i] = l;
+    AL[i] = a;
+    Z[i] = heat_stencil_cell(x, y, X, Y, g) ? mul(dt, mul(a, l)) : 0.0f;
+  }
+  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
+    const int lx = i / OY, ly = i - lx * OY;
+    GA[i] = P.galpha[(size_t)(bx0 + lx) * Y + by0 + ly];
+  }
+  __syncthreads();
+  const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
+  const int lxs = (int)threadIdx.x / RY, lys = (int)threadIdx.x - lxs * RY;
+  for (int s = 0; s < P.k; ++s) {
+    const float* Sn = P.lsts + (size_t)(P.ntop - s) * P.cells;
+    // mu = lam + L^T(z); the gradient term of step n on the tile
+    int lx = lxs, ly = lys;
+    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int t = 0; t < 2 * R + 1; ++t) {
+        const int nx = lx + t - R;
+        const float zv = (nx >= 0 && nx < RX) ? Z[i + (t - R) * RY] : 0.0f;
+        acc = add(acc, mul(P.w[t], zv));
+      }
+#pragma unroll
+      for (int t = 0; t < 2 * R + 1; ++t) {
+        const int ny = ly + t - R;
+        const float zv = (ny >= 0 && ny < RY) ? Z[i + (t - R)] : 0.0f;
+        acc = add(acc, mul(P.w[t], zv));
+      }
+      const float l = Lm[i];
+      M[i] = add(l, acc);
+      const int x = rx0 + lx, y = ry0 + ly;
+      if (x >= bx0 && x < ox1 && y >= by0 && y < oy1 && heat_stencil_cell(x, y, X, Y, g)) {
+        const int gi = (x - bx0) * OY + (y - by0);
+        GA[gi] = add(GA[gi], mul(l, mul(dt, __ldg(Sn + (size_t)x * Y + y))));
+      }
+      lx += dq;
+      ly += dr;
+      if (ly >= RY) { ly -= RY; ++lx; }
+    }
+    __syncthreads();
+    // lam = B^T(mu); z for the next step
+    lx = lxs;
+    ly = lys;
+    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+      const int x = rx0 + lx, y = ry0 + ly;
+      float v = bc_overwritten(Rl, x, y, X, Y, g) ? 0.0f : M[i];
+      const bool yin = y >= g && y < Y - g, xin = x >= g && x < X - g;
+      // the ghost of each pair lies in the region whenever its partner does (edge snapping)
+      if (yin && x == g + 1) v = bt_ghost(Rl, v, M[i - 2 * RY], g, y, 0, X, Y, g);
+      if (yin && x == X - g - 2) v = bt_ghost(Rl, v, M[i + 2 * RY], X - g - 1, y, 0, X, Y, g);
+      if (xin && y == g + 1) v = bt_ghost(Rl, v, M[i - 2], x, g, 1, X, Y, g);
+      if (xin && y == Y - g - 2) v = bt_ghost(Rl, v, M[i + 2], x, Y - g - 1, 1, X, Y, g);
+      Lm[i] = v;
+      Z[i] = heat_stencil_cell(x, y, X, Y, g) ? mul(dt, mul(AL[i], v)) : 0.0f;
+      lx += dq;
+      ly += dr;
+      if (ly >= RY) { ly -= RY; ++lx; }
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
+    const int lx = i / OY, ly = i - lx * OY;
+    const size_t gi = (size_t)(bx0 + lx) * Y + by0 + ly;
+    lam_out[gi] = Lm[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+    P.galpha[gi] = GA[i];
+  }
+}
+
+}  // namespace pde

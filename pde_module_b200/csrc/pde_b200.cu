@@ -11,6 +11,7 @@
 #include "ldc.cuh"
 #include "wave.cuh"
 #include "batched.cuh"
+#include "heat_adj.cuh"
 
 using namespace pde;
 
@@ -533,6 +534,136 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
   if (need_copy) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, work, bytes, cudaMemcpyDeviceToDevice, st));
   return PDE_OK;
 }
+
+namespace {
+
+constexpr int HA_TBX = 32, HA_TBY = 64;
+
+// Shared checks and launch geometry of the differentiable heat entry points.
+int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_pass, int nsteps, Geo* G,
+                    HAParams* P, int* kk) {
+  if (!make_geo(grid, G)) return PDE_ERR_SHAPE;
+  if (G->ndims != 2 || G->n[2] != 1) return PDE_ERR_UNSUPPORTED;
+  if (G->g < G->order / 2 || G->g < 1) return PDE_ERR_GHOST;
+  if (rules->ncomp != 1) return PDE_ERR_ARG;
+  if (rules->has_ramp) return PDE_ERR_UNSUPPORTED;
+  if (G->n[0] < 2 * G->g + 3 || G->n[1] < 2 * G->g + 3) return PDE_ERR_SHAPE;
+  const Weights W = lap_weights(G->order, grid->dx);
+  memset(P, 0, sizeof(*P));
+  P->X = (int)G->n[0];
+  P->Y = (int)G->n[1];
+  P->g = G->g;
+  for (int t = 0; t < 5; ++t) P->w[t] = W.w[t];
+  int k = steps_per_pass > 0 ? steps_per_pass : 8;
+  if (k > nsteps) k = nsteps;
+  if (k < 1) k = 1;
+  *kk = k;
+  P->TBX = HA_TBX;
+  P->TBY = HA_TBY;
+  P->tiles_y = (P->Y + P->TBY - 1) / P->TBY;
+  P->cells = (long long)G->n[0] * G->n[1];
+  return PDE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                     const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
+                     void* stream) {
+  if (!alpha || !u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
+  if (work == u_in || work == u_out) return PDE_ERR_ARG;
+  Geo G;
+  HAParams P;
+  int k;
+  int rc = heat_diff_setup(grid, rules, steps_per_pass, nsteps, &G, &P, &k);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = (size_t)P.cells * sizeof(float);
+  if (nsteps == 0) {
+    if (u_out != u_in) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, u_in, bytes, cudaMemcpyDeviceToDevice, st));
+    return PDE_OK;
+  }
+  const int R = G.order / 2;
+  const int H = k * R + 1;
+  P.RC = (P.TBX + 2 * H) * (P.TBY + 2 * H);
+  const size_t smem = (size_t)3 * P.RC * sizeof(float);
+  if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  auto kern = R == 1 ? heat2d_field_fwd_kernel<1> : heat2d_field_fwd_kernel<2>;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  P.alpha = alpha;
+  P.dt = dt;
+  const int npasses = (nsteps + k - 1) / k;
+  const bool alias = (u_out == u_in);
+  const float* src = u_in;
+  float* dst = alias ? work : ((npasses % 2 == 1) ? u_out : work);
+  int done = 0;
+  for (int p = 0; p < npasses; ++p) {
+    P.k = (nsteps - done < k) ? (nsteps - done) : k;
+    P.lst = lstates ? lstates + (size_t)done * P.cells : nullptr;
+    kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);
+    rc = launch_status();
+    if (rc) return rc;
+    done += P.k;
+    src = dst;
+    dst = (dst == work) ? u_out : work;
+  }
+  if (src != u_out) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, src, bytes, cudaMemcpyDeviceToDevice, st));
+  return PDE_OK;
+}
+
+int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, const float* lstates,
+                     float* grad_alpha, const PdeGrid* grid, const PdeBCRules* rules, float dt, int32_t nsteps,
+                     int32_t steps_per_pass, float* work, void* stream) {
+  if (!alpha || !lam_in || !lam_out || !lstates || !grad_alpha || !work || !grid || !rules || nsteps < 0 ||
+      steps_per_pass < 0)
+    return PDE_ERR_ARG;
+  if (work == lam_in || work == lam_out) return PDE_ERR_ARG;
+  Geo G;
+  HAParams P;
+  int k;
+  int rc = heat_diff_setup(grid, rules, steps_per_pass, nsteps, &G, &P, &k);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = (size_t)P.cells * sizeof(float);
+  if (nsteps == 0) {
+    if (lam_out != lam_in) PDE_CUDA_CHECK(cudaMemcpyAsync(lam_out, lam_in, bytes, cudaMemcpyDeviceToDevice, st));
+    return PDE_OK;
+  }
+  const int R = G.order / 2;
+  const int H = k * R;
+  P.RC = (P.TBX + 2 * H + 2 * (G.g + 2)) * (P.TBY + 2 * H + 2 * (G.g + 2));
+  const size_t smem = ((size_t)4 * P.RC + (size_t)P.TBX * P.TBY) * sizeof(float);
+  if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  auto kern = R == 1 ? heat2d_adj_kernel<1> : heat2d_adj_kernel<2>;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  P.alpha = alpha;
+  P.dt = dt;
+  P.lsts = lstates;
+  P.galpha = grad_alpha;
+  const int npasses = (nsteps + k - 1) / k;
+  const bool alias = (lam_out == lam_in);
+  const float* src = lam_in;
+  float* dst = alias ? work : ((npasses % 2 == 1) ? lam_out : work);
+  int done = 0;
+  for (int p = 0; p < npasses; ++p) {
+    P.k = (nsteps - done < k) ? (nsteps - done) : k;
+    P.ntop = nsteps - 1 - done;
+    kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);
+    rc = launch_status();
+    if (rc) return rc;
+    done += P.k;
+    src = dst;
+    dst = (dst == work) ? lam_out : work;
+  }
+  if (src != lam_out) PDE_CUDA_CHECK(cudaMemcpyAsync(lam_out, src, bytes, cudaMemcpyDeviceToDevice, st));
+  return PDE_OK;
+}
+
+}  // extern "C"
 
 namespace {
 
