@@ -390,6 +390,10 @@ def exchange_x_halos(f, g, rank, world):
     f[n - g:n].copy_(recv_hi)
 
 
+# output tiles tried for the temporally blocked 2D kernels ((0, 0): the library's automatic choice)
+TILES_2D = ((0, 0), (32, 64), (32, 32), (16, 32), (16, 64))
+
+
 def run_heat(steps: int = 1000):
     """2D heat, 256^2 interior + 1 ghost, Dirichlet 0, alpha 1, dt = 0.2 dx^2, u0 =
     U[0,1) (seed 0) x Gaussian bump (sigma 0.1): the fused rollout (boundary fill +
@@ -455,8 +459,10 @@ def run_heat(steps: int = 1000):
     cells = n * n * steps
     # differentiable form: alpha as a field, gradients w.r.t. alpha and u0 by the adjoint
     # with sqrt(N) checkpoints; loss = mean squared final field
+    import pde_module_b200._lib as L
     adj = {}
-    for k in (4, 8, 16):
+    for tile, k in [(t, q) for t in TILES_2D for q in (4, 8, 16)]:
+        L.check(L.lib().pde_set_tile_2d(*tile), "pde_set_tile_2d")
         solver = P.HeatSolver(bc, dx, dt, steps, steps_per_pass=k)
         a_f = torch.ones_like(u0)
 
@@ -483,22 +489,26 @@ def run_heat(steps: int = 1000):
             return e0.elapsed_time(e1) / reps
 
         f_ms, fa_ms = ev(fwd), ev(fwd_adj)
-        adj[k] = (f_ms, fa_ms)
+        adj[(tile, k)] = (f_ms, fa_ms)
     kb = min(adj, key=lambda q: adj[q][1])
-    same_fwd = bool(torch.equal(P.HeatSolver(bc, dx, dt, steps, steps_per_pass=kb).forward(torch.ones_like(u0), u0),
-                                out_chain))
+    L.check(L.lib().pde_set_tile_2d(*kb[0]), "pde_set_tile_2d")
+    same_fwd = bool(torch.equal(P.HeatSolver(bc, dx, dt, steps, steps_per_pass=kb[1]).forward(torch.ones_like(u0),
+                                                                                             u0), out_chain))
+    L.check(L.lib().pde_set_tile_2d(0, 0), "pde_set_tile_2d")
     return {"workload": "2D heat 256^2, Dirichlet 0, 1000 steps (examples/2D_Heat_Equation.py loop)",
             "fused_cell_updates_per_s": cells / (best[0] / 1000.0), "fused_k": best[1],
             "chain_cell_updates_per_s": cells / (res["chain_ms"] / 1000.0),
             "speedup_vs_chain": res["chain_ms"] / best[0],
             "bitwise_equal_to_chain": bool(torch.equal(best[2], out_chain)),
             "times_ms": {k: round(v, 4) for k, v in res.items()},
-            "adjoint": {"steps_per_pass": kb, "forward_ms": adj[kb][0], "forward_adjoint_ms": adj[kb][1],
+            "adjoint": {"steps_per_pass": kb[1], "tile": list(kb[0]) if kb[0] != (0, 0) else "auto",
+                        "forward_ms": adj[kb][0], "forward_adjoint_ms": adj[kb][1],
                         "ratio_fwd_adj_over_fwd": adj[kb][1] / adj[kb][0],
                         "forward_bitwise_equal_to_chain": same_fwd,
-                        "by_k": {str(q): [round(v[0], 4), round(v[1], 4)] for q, v in adj.items()},
+                        "by_tile_k": {f"{q[0][0]}x{q[0][1]}_k{q[1]}": [round(v[0], 4), round(v[1], 4)]
+                                      for q, v in adj.items()},
                         "note": "alpha as a field, grads w.r.t. alpha and u0, sqrt(N) checkpoints (every 32 "
-                                "steps), eager launches (no graph)"},
+                                "steps), forward and backward each replayed as one CUDA graph"},
             "note": "both as CUDA graph replays; the working set (0.27 MB) is L2-resident, launch-bound"}
 
 
@@ -579,23 +589,26 @@ def run_wave(n: int = 512, steps: int = 2000):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps, out
 
+    import pde_module_b200._lib as L
     best = None
-    for k in (4, 8, 12, 16):
-        solver.steps_per_pass = k
-        ms, _ = timed(fwd_adj, 1)
-        if best is None or ms < best[0]:
-            best = (ms, k)
+    for tile in TILES_2D:
+        L.check(L.lib().pde_set_tile_2d(*tile), "pde_set_tile_2d")
+        for k in (4, 8, 12, 16):
+            solver.steps_per_pass = k  # also drops the captured graphs
+            ms, _ = timed(fwd_adj, 1)
+            if best is None or ms < best[0]:
+                best = (ms, k, tile)
+    L.check(L.lib().pde_set_tile_2d(*best[2]), "pde_set_tile_2d")
     solver.steps_per_pass = best[1]
     f_ms, _ = timed(fwd_only)
     fa_ms, (loss, gc, gu) = timed(fwd_adj)
     # the same with every state kept (one segment: no recomputation; 2000 x 1 MB)
     every = solver.every
-    solver.every = steps
-    solver._work = None
+    solver.set_checkpoint_every(steps)
     fa_all_ms, (loss2, gc2, _) = timed(fwd_adj)
-    solver.every = every
-    solver._work = None
+    solver.set_checkpoint_every(every)
     same = bool(torch.equal(gc, gc2))
+    L.check(L.lib().pde_set_tile_2d(0, 0), "pde_set_tile_2d")
     cells = n * n * steps
     return {"workload": f"differentiable wave {n}^2, {steps} leapfrog steps, CFL 0.5, Ricker source, "
                         f"MSE vs target, grads w.r.t. speed and initial field, sqrt(N) checkpoints "
@@ -604,6 +617,7 @@ def run_wave(n: int = 512, steps: int = 2000):
             "store_all_states": {"forward_adjoint_ms": fa_all_ms, "ratio_fwd_adj_over_fwd": fa_all_ms / f_ms,
                                  "grad_bitwise_equal_to_checkpointed": same},
             "forward_cell_updates_per_s": cells / (f_ms / 1000.0), "steps_per_pass": best[1],
+            "tile": list(best[2]) if best[2] != (0, 0) else "auto",
             "loss": float(loss.item()), "grad_c_norm": float(gc.norm().item()),
             "grad_u0_norm": float(gu.norm().item())}
 

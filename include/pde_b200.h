@@ -272,19 +272,25 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
  *   u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) + src[n] at src_cell
  * pde_wave_forward: nsteps from (u^{n0-1}, u^{n0}) = (u_prev, u_cur) to
  * (out_prev, out_cur) = (u^{n0+nsteps-1}, u^{n0+nsteps}); src_cell < 0: no source.
- * states (NULL or nsteps fields): states[j] = u^{n0+1+j}.  work: 2 fields.
+ * lstates (NULL or nsteps fields): lstates[j] = L(u^{n0+j}) on the cells inside
+ * the node ring, 0 elsewhere (the Laplacian each step forms).  work: 2 fields.
  * steps_per_pass: temporal-blocking depth (0 = 8). */
 int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, float* out_prev, float* out_cur,
                      const float* src, int64_t src_cell, int32_t n0, int32_t nsteps, int32_t steps_per_pass,
-                     float* states, float* work, const PdeGrid* grid, void* stream);
-/* Discrete adjoint over steps n = nsteps-1 .. 0 of a segment whose states are
- * ustates[j] = u^j (j = 0 .. nsteps-1):  mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1}),
- * grad_K += mu^{n+1} o L(u^n) (read-modify-write once per step, n descending).
+                     float* lstates, float* work, const PdeGrid* grid, void* stream);
+/* Discrete adjoint over steps n = nsteps-1 .. 0 of a segment whose forward wrote
+ * lstates[j] = L(u^j) (j = 0 .. nsteps-1):  mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1}),
+ * grad_K += mu^{n+1} o L(u^n) (one add per cell and step, n descending).
  * In: (mu_next, mu_next2) = (mu^{nsteps}, mu^{nsteps+1}); out: (mu_out, mu_out_next) =
  * (mu^0, mu^1).  work: 2 fields. */
 int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out,
-                     float* mu_out_next, const float* ustates, float* grad_K, int32_t nsteps,
+                     float* mu_out_next, const float* lstates, float* grad_K, int32_t nsteps,
                      int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
+/* Output tile (cells) of the temporally blocked 2D kernels of pde_heat_forward,
+ * pde_heat_adjoint, pde_wave_forward and pde_wave_adjoint, process-wide; (0, 0)
+ * restores the automatic choice (the largest of 32x64, 32x32, 16x32 that gives
+ * every SM a tile).  Sides 8..256. */
+int pde_set_tile_2d(int32_t tile_x, int32_t tile_y);
 
 /* ---- batched rollouts (new: the reference advances every grid with its own
  * module chain, examples/2D_Heat_Equation.py:57-65, three launches per step

@@ -537,7 +537,27 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
 
 namespace {
 
-constexpr int HA_TBX = 32, HA_TBY = 64;
+// Output tile of the temporally blocked 2D kernels (differentiable heat, wave):
+// the largest of 32x64, 32x32, 16x32 that still gives every SM a tile, unless
+// pde_set_tile_2d fixed one.
+int g_tile2d[2] = {0, 0};
+
+void pick_tile_2d(int X, int Y, int* tbx, int* tby) {
+  if (g_tile2d[0] > 0) {
+    *tbx = g_tile2d[0];
+    *tby = g_tile2d[1];
+    return;
+  }
+  static const int cand[3][2] = {{32, 64}, {32, 32}, {16, 32}};
+  for (int c = 0; c < 3; ++c) {
+    const long long tiles = (long long)((X + cand[c][0] - 1) / cand[c][0]) * ((Y + cand[c][1] - 1) / cand[c][1]);
+    if (tiles >= sm_count() || c == 2) {
+      *tbx = cand[c][0];
+      *tby = cand[c][1];
+      return;
+    }
+  }
+}
 
 // Shared checks and launch geometry of the differentiable heat entry points.
 int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_pass, int nsteps, Geo* G,
@@ -558,8 +578,7 @@ int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_
   if (k > nsteps) k = nsteps;
   if (k < 1) k = 1;
   *kk = k;
-  P->TBX = HA_TBX;
-  P->TBY = HA_TBY;
+  pick_tile_2d(P->X, P->Y, &P->TBX, &P->TBY);
   P->tiles_y = (P->Y + P->TBY - 1) / P->TBY;
   P->cells = (long long)G->n[0] * G->n[1];
   return PDE_OK;
@@ -568,6 +587,17 @@ int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_
 }  // namespace
 
 extern "C" {
+
+int pde_set_tile_2d(int32_t tile_x, int32_t tile_y) {
+  if (tile_x == 0 && tile_y == 0) {
+    g_tile2d[0] = g_tile2d[1] = 0;
+    return PDE_OK;
+  }
+  if (tile_x < 8 || tile_y < 8 || tile_x > 256 || tile_y > 256) return PDE_ERR_ARG;
+  g_tile2d[0] = tile_x;
+  g_tile2d[1] = tile_y;
+  return PDE_OK;
+}
 
 int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
                      const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
@@ -668,7 +698,7 @@ int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, co
 namespace {
 
 bool wave_setup(const PdeGrid* grid, int steps_per_pass, int nsteps, Geo* G, WaveParams* P, int* kk, size_t* smem,
-                int nbuf) {
+                int nbuf, int extra) {
   if (!make_geo(grid, G)) return false;
   if (G->ndims != 2 || G->n[2] != 1 || grid->order != 2 || G->g < 1) return false;
   const Weights WL = lap_weights(2, grid->dx);
@@ -681,14 +711,12 @@ bool wave_setup(const PdeGrid* grid, int steps_per_pass, int nsteps, Geo* G, Wav
   if (k > nsteps) k = nsteps;
   if (k < 1) k = 1;
   *kk = k;
-  P->TBX = WAVE_TBX;
-  P->TBY = WAVE_TBY;
+  pick_tile_2d(P->X, P->Y, &P->TBX, &P->TBY);
   P->tiles_y = (P->Y + P->TBY - 1) / P->TBY;
-  P->RXM = P->TBX + 2 * k;
-  P->RYM = P->TBY + 2 * k;
+  P->RC = (P->TBX + 2 * k) * (P->TBY + 2 * k);
   P->cells = (long long)G->n[0] * G->n[1];
   P->srcx = -1;
-  *smem = (size_t)nbuf * P->RXM * P->RYM * sizeof(float);
+  *smem = ((size_t)nbuf * P->RC + (size_t)extra * P->TBX * P->TBY) * sizeof(float);
   return *smem <= 227 * 1024;
 }
 
@@ -696,14 +724,14 @@ bool wave_setup(const PdeGrid* grid, int steps_per_pass, int nsteps, Geo* G, Wav
 
 int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, float* out_prev, float* out_cur,
                      const float* src, int64_t src_cell, int32_t n0, int32_t nsteps, int32_t steps_per_pass,
-                     float* states, float* work, const PdeGrid* grid, void* stream) {
+                     float* lstates, float* work, const PdeGrid* grid, void* stream) {
   if (!K || !u_prev || !u_cur || !out_prev || !out_cur || !work || !grid || nsteps < 0 || n0 < 0) return PDE_ERR_ARG;
   if (src_cell >= 0 && !src) return PDE_ERR_ARG;
   Geo G;
   WaveParams P;
   int k;
   size_t smem;
-  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 4)) return PDE_ERR_UNSUPPORTED;
+  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 4, 0)) return PDE_ERR_UNSUPPORTED;
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)P.cells;
   if (nsteps == 0) {
@@ -730,7 +758,7 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
   for (int p = 0; p < npasses; ++p) {
     P.k = (nsteps - done < k) ? (nsteps - done) : k;
     P.n0 = n0 + done;
-    P.states = states ? states + (size_t)done * P.cells : nullptr;
+    P.lst = lstates ? lstates + (size_t)done * P.cells : nullptr;
     float* da = to_out ? out_prev : w0;
     float* db = to_out ? out_cur : w1;
     wave_fwd_tb_kernel<<<tiles, 256, smem, st>>>(a, b, K, da, db, P);
@@ -749,16 +777,16 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
 }
 
 int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out, float* mu_out_next,
-                     const float* ustates, float* grad_K, int32_t nsteps, int32_t steps_per_pass, float* work,
+                     const float* lstates, float* grad_K, int32_t nsteps, int32_t steps_per_pass, float* work,
                      const PdeGrid* grid, void* stream) {
-  if (!K || !mu_next || !mu_next2 || !mu_out || !mu_out_next || !ustates || !grad_K || !work || !grid ||
+  if (!K || !mu_next || !mu_next2 || !mu_out || !mu_out_next || !lstates || !grad_K || !work || !grid ||
       nsteps < 1)
     return PDE_ERR_ARG;
   Geo G;
   WaveParams P;
   int k;
   size_t smem;
-  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 4)) return PDE_ERR_UNSUPPORTED;
+  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 6, 1)) return PDE_ERR_UNSUPPORTED;
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)P.cells;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_adj_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -770,8 +798,7 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
   bool to_out = alias ? false : (npasses % 2 == 1);
   const float* a = mu_next;
   const float* b = mu_next2;
-  P.ustates = ustates;
-  P.ubase = 0;  // ustates[j] = u^{nbot + j}; steps are numbered from nbot = 0 here
+  P.lsts = lstates;  // lstates[n] = L(u^n), steps numbered from 0 within the segment
   P.gK = grad_K;
   int done = 0;
   for (int p = 0; p < npasses; ++p) {

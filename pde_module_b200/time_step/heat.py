@@ -18,6 +18,7 @@ import torch
 
 from .._lib import lib, check, stream_ptr, require_cuda_f32, make_grid
 from ..FDM.boundary import GridBoundary
+from ._replay import GraphedSequence
 
 
 class HeatRollout:
@@ -60,13 +61,14 @@ class HeatSolver:
 
     which is the module chain's step with alpha taken per cell (bit-identical to
     ``HeatRollout`` for a constant field).  ``forward`` keeps ceil(sqrt(N))
-    checkpoints of u; ``backward`` recomputes each segment's S from its checkpoint
-    (the last segment keeps them from the forward pass) and runs the discrete
-    adjoint, returning (dJ/dalpha, dJ/du0)."""
+    checkpoints of u and the last segment's S; ``backward`` recomputes every
+    other segment's S from its checkpoint and runs the discrete adjoint,
+    returning (dJ/dalpha, dJ/du0).  Buffers are allocated once per device; with
+    ``graphs`` (default) each sequence is captured as a CUDA graph after its first
+    run and replayed afterwards.  One backward() belongs to the latest forward()."""
 
     def __init__(self, boundary: GridBoundary, dx: float, dt: float, nsteps: int, order: int = 2,
-                 steps_per_pass: int = 0, checkpoint_every: int | None = None) -> None:
-        import math
+                 steps_per_pass: int = 0, checkpoint_every: int | None = None, graphs: bool = True) -> None:
         if boundary.inputs[0] != 1:
             raise ValueError("HeatSolver takes scalar fields")
         self.boundary = boundary
@@ -75,17 +77,46 @@ class HeatSolver:
         self.dx, self.dt, self.N, self.order = float(dx), float(dt), int(nsteps), int(order)
         self.rules = boundary.rules()
         self.grid = make_grid(self.shape, boundary.ghost_cells, self.order, self.dx)
-        self.steps_per_pass = int(steps_per_pass)
-        self.every = int(checkpoint_every) if checkpoint_every else max(1, int(math.ceil(math.sqrt(self.N))))
-        self.checkpoints = []
-        self._work = None
-        self._last_seg_ready = False
+        self._steps_per_pass = int(steps_per_pass)
+        self.graphs = bool(graphs)
+        self.set_checkpoint_every(checkpoint_every)
+
+    def set_checkpoint_every(self, every: int | None) -> None:
+        """Checkpoint spacing (None: ceil(sqrt(N))); frees the buffers and graphs."""
+        import math
+        self.every = int(every) if every else max(1, int(math.ceil(math.sqrt(self.N))))
+        self.segments = [(n0, min(self.every, self.N - n0)) for n0 in range(0, self.N, self.every)]
+        self._dev = None
+        self._seq_f = GraphedSequence(self._run_forward, self.graphs)
+        self._seq_b = GraphedSequence(self._run_backward, self.graphs)
+
+    @property
+    def steps_per_pass(self) -> int:
+        return self._steps_per_pass
+
+    @steps_per_pass.setter
+    def steps_per_pass(self, k: int) -> None:
+        self._steps_per_pass = int(k)
+        self._seq_f.reset()
+        self._seq_b.reset()
 
     def _buffers(self, like: torch.Tensor) -> None:
-        if self._work is None or self._work.device != like.device:
-            cells = self.shape[0] * self.shape[1]
-            self._work = torch.zeros(cells, dtype=torch.float32, device=like.device)
-            self._seg = torch.zeros((self.every, cells), dtype=torch.float32, device=like.device)
+        if self._dev == like.device:
+            return
+        dev, f = like.device, self.shape + (1,)
+        cells = self.shape[0] * self.shape[1]
+        z = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)
+        self._work = z(cells)
+        self._seg = z(max(self.every, 1), cells)
+        self._alpha, self._g = z(*f), z(*f)
+        self._ck = z(max(len(self.segments), 1), *f)  # u^{n0} per segment
+        self._out = z(*f)
+        self._lam = z(2, *f)
+        self._tmp = z(*f)
+        self._ga = z(*f)
+        self._dev = dev
+        self._seq_f.reset()
+        self._seq_b.reset()
 
     def _fwd(self, alpha, u, out, nsteps, lstates=None):
         check(lib().pde_heat_forward(C.c_void_p(alpha.data_ptr()), C.c_void_p(u.data_ptr()),
@@ -101,46 +132,50 @@ class HeatSolver:
         if tuple(alpha.shape) != self.shape + (1,) or tuple(u.shape) != self.shape + (1,):
             raise AssertionError(f"alpha and u must be {self.shape + (1,)}")
 
+    def _run_forward(self) -> None:
+        for j, (n0, m) in enumerate(self.segments):
+            last = j == len(self.segments) - 1
+            self._fwd(self._alpha, self._ck[j], self._out if last else self._ck[j + 1], m,
+                      self._seg[:m] if last else None)
+        if not self.segments:
+            self._out.copy_(self._ck[0])
+
+    def _run_backward(self) -> None:
+        self._ga.zero_()
+        a, b = self._lam[0], self._lam[1]
+        a.copy_(self._g)
+        for j in range(len(self.segments) - 1, -1, -1):
+            n0, m = self.segments[j]
+            seg = self._seg[:m]
+            if j != len(self.segments) - 1:  # recompute S^{n0} .. S^{n0+m-1} from the checkpoint
+                self._fwd(self._alpha, self._ck[j], self._tmp, m, seg)
+            check(lib().pde_heat_adjoint(C.c_void_p(self._alpha.data_ptr()), C.c_void_p(a.data_ptr()),
+                                         C.c_void_p(b.data_ptr()), C.c_void_p(seg.data_ptr()),
+                                         C.c_void_p(self._ga.data_ptr()), C.byref(self.grid), C.byref(self.rules),
+                                         self.dt, m, self.steps_per_pass, C.c_void_p(self._work.data_ptr()),
+                                         C.c_void_p(stream_ptr(a))), "pde_heat_adjoint")
+            a, b = b, a
+
     def forward(self, alpha: torch.Tensor, u0: torch.Tensor) -> torch.Tensor:
-        """u^N; keeps u at n = 0, every, 2*every, ... and the last segment's S."""
+        """u^N for diffusivity field alpha and initial field u0."""
         self._check(alpha, u0)
         self._buffers(u0)
-        self.checkpoints = []
-        self._last_seg_ready = False
-        cur, n = u0, 0
-        while n < self.N:
-            self.checkpoints.append((n, cur.clone()))
-            m = min(self.every, self.N - n)
-            out = torch.empty_like(cur)
-            last = n + m == self.N
-            self._fwd(alpha, cur, out, m, self._seg[:m] if last else None)
-            self._last_seg_ready = last
-            cur, n = out, n + m
-        if self.N == 0:
-            cur = u0.clone()
-        return cur
+        self._alpha.copy_(alpha)
+        self._ck[0].copy_(u0)
+        self._seq_f.run()
+        self._fwd_done = True
+        return self._out.clone()
 
     def backward(self, alpha: torch.Tensor, dJ_duN: torch.Tensor):
         """(dJ/dalpha, dJ/du0) for the last forward()."""
-        lam = dJ_duN.contiguous()
-        self._check(alpha, lam)
-        self._buffers(alpha)
-        galpha = torch.zeros_like(alpha)
-        kept, self._last_seg_ready = self._last_seg_ready, False
-        scratch = torch.empty_like(lam)
-        for n0, u in reversed(self.checkpoints):
-            m = min(self.every, self.N - n0)
-            seg = self._seg[:m]
-            if not (kept and n0 + m == self.N):
-                self._fwd(alpha, u, scratch, m, seg)  # recompute S^{n0} .. S^{n0+m-1}
-            out = torch.empty_like(lam)
-            check(lib().pde_heat_adjoint(C.c_void_p(alpha.data_ptr()), C.c_void_p(lam.data_ptr()),
-                                         C.c_void_p(out.data_ptr()), C.c_void_p(seg.data_ptr()),
-                                         C.c_void_p(galpha.data_ptr()), C.byref(self.grid), C.byref(self.rules),
-                                         self.dt, m, self.steps_per_pass, C.c_void_p(self._work.data_ptr()),
-                                         C.c_void_p(stream_ptr(lam))), "pde_heat_adjoint")
-            lam = out
-        return galpha, lam.clone() if lam is dJ_duN else lam
+        if not getattr(self, "_fwd_done", False):
+            raise RuntimeError("backward() needs a forward() first")
+        self._check(alpha, dJ_duN.contiguous())
+        self._alpha.copy_(alpha)
+        self._g.copy_(dJ_duN)
+        self._seq_b.run()
+        gu = self._lam[len(self.segments) % 2]  # the buffer the last adjoint pass wrote
+        return self._ga.clone(), gu.clone()
 
 
 class _HeatFn(torch.autograd.Function):

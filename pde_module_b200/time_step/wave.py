@@ -22,11 +22,21 @@ import numpy as np
 import torch
 
 from .._lib import lib, check, stream_ptr, make_grid, require_cuda_f32
+from ._replay import GraphedSequence
 
 
 class WaveSolver:
+    """Leapfrog rollout of N steps and its adjoint with sqrt(N) checkpoints.
+
+    All buffers are allocated once per device: checkpoints (u^{n-1}, u^n) at the
+    start of every segment, L(u^n) of one segment, the adjoint's mu pairs.  With
+    ``graphs`` (default) the forward and the backward sequences are each captured
+    as a CUDA graph after their first (eager) run and replayed afterwards.  One
+    backward() belongs to the latest forward()."""
+
     def __init__(self, shape, dx: float, nsteps: int, src: torch.Tensor | None = None, src_cell=None,
-                 ghost_cells: int = 1, steps_per_pass: int = 0, checkpoint_every: int | None = None) -> None:
+                 ghost_cells: int = 1, steps_per_pass: int = 0, checkpoint_every: int | None = None,
+                 graphs: bool = True) -> None:
         self.shape = tuple(int(s) for s in shape[:3])
         assert self.shape[2] == 1, "2D grids (X, Y, 1)"
         self.dx, self.N, self.g = float(dx), int(nsteps), int(ghost_cells)
@@ -41,77 +51,109 @@ class WaveSolver:
         if self.src_cell >= 0:
             require_cuda_f32(src, "src")
             assert src.numel() >= self.N
-        self.steps_per_pass = int(steps_per_pass)
-        self.every = int(checkpoint_every) if checkpoint_every else max(1, int(math.ceil(math.sqrt(self.N))))
-        self.checkpoints = []
-        self._work = None
+        self._steps_per_pass = int(steps_per_pass)
+        self.graphs = bool(graphs)
+        self.set_checkpoint_every(checkpoint_every)
 
-    def _buffers(self, like: torch.Tensor):
-        if self._work is None or self._work.device != like.device:
-            cells = self.shape[0] * self.shape[1]
-            self._work = torch.zeros((2, cells), dtype=torch.float32, device=like.device)
-            self._seg = torch.zeros((self.every + 1, cells), dtype=torch.float32, device=like.device)
-        self._last_seg_ready = getattr(self, "_last_seg_ready", False)
+    # -- configuration ---------------------------------------------------------
+    def set_checkpoint_every(self, every: int | None) -> None:
+        """Checkpoint spacing (None: ceil(sqrt(N))); frees the buffers and graphs."""
+        self.every = int(every) if every else max(1, int(math.ceil(math.sqrt(self.N))))
+        self.segments = [(n0, min(self.every, self.N - n0)) for n0 in range(0, self.N, self.every)]
+        self._dev = None
+        self._seq_f = GraphedSequence(self._run_forward, self.graphs)
+        self._seq_b = GraphedSequence(self._run_backward, self.graphs)
 
-    def _fwd(self, K, a, b, oa, ob, n0, nsteps, states=None):
+    @property
+    def steps_per_pass(self) -> int:
+        return self._steps_per_pass
+
+    @steps_per_pass.setter
+    def steps_per_pass(self, k: int) -> None:
+        self._steps_per_pass = int(k)
+        self._seq_f.reset()
+        self._seq_b.reset()
+
+    def _buffers(self, like: torch.Tensor) -> None:
+        if self._dev == like.device:
+            return
+        dev, f = like.device, self.shape + (1,)
+        z = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)
+        self._work = z(2, self.shape[0] * self.shape[1])
+        self._seg = z(max(self.every, 1), self.shape[0] * self.shape[1])
+        self._K, self._u0, self._g = z(*f), z(*f), z(*f)
+        self._ck = z(max(len(self.segments), 1), 2, *f)       # (u^{n0-1}, u^{n0}) per segment
+        self._out = z(2, *f)                                   # (u^{N-1}, u^N)
+        self._mu = z(2, 2, *f)                                 # ping-pong (mu^{n+1}, mu^{n+2}) pairs
+        self._tmp = z(2, *f)
+        self._gK, self._gu = z(*f), z(*f)
+        self._mask = interior_mask(self.shape, self.g, dev)
+        self._dev = dev
+        self._seq_f.reset()
+        self._seq_b.reset()
+
+    def _fwd(self, K, a, b, oa, ob, n0, nsteps, lstates=None):
         check(lib().pde_wave_forward(C.c_void_p(K.data_ptr()), C.c_void_p(a.data_ptr()), C.c_void_p(b.data_ptr()),
                                      C.c_void_p(oa.data_ptr()), C.c_void_p(ob.data_ptr()),
                                      C.c_void_p(self.src.data_ptr()) if self.src_cell >= 0 else None,
                                      self.src_cell, n0, nsteps, self.steps_per_pass,
-                                     C.c_void_p(states.data_ptr()) if states is not None else None,
+                                     C.c_void_p(lstates.data_ptr()) if lstates is not None else None,
                                      C.c_void_p(self._work.data_ptr()), C.byref(self.grid),
                                      C.c_void_p(stream_ptr(K))), "pde_wave_forward")
 
+    # -- the two launch sequences (static buffers only) ------------------------
+    def _run_forward(self) -> None:
+        self._ck[0, 0].copy_(self._u0)
+        self._ck[0, 1].copy_(self._u0)
+        for j, (n0, m) in enumerate(self.segments):
+            last = j == len(self.segments) - 1
+            o = self._out if last else self._ck[j + 1]
+            # the last segment keeps L(u^n): the adjoint starts there without recomputing
+            self._fwd(self._K, self._ck[j, 0], self._ck[j, 1], o[0], o[1], n0, m,
+                      lstates=self._seg[:m] if last else None)
+        if not self.segments:
+            self._out[0].copy_(self._u0)
+            self._out[1].copy_(self._u0)
+
+    def _run_backward(self) -> None:
+        self._gK.zero_()
+        a, b = self._mu[0], self._mu[1]
+        a[0].copy_(self._g)
+        a[1].zero_()
+        for j in range(len(self.segments) - 1, -1, -1):
+            n0, m = self.segments[j]
+            seg = self._seg[:m]
+            if j != len(self.segments) - 1:  # recompute L(u^{n0}) .. L(u^{n0+m-1}) from the checkpoint
+                self._fwd(self._K, self._ck[j, 0], self._ck[j, 1], self._tmp[0], self._tmp[1], n0, m, lstates=seg)
+            check(lib().pde_wave_adjoint(C.c_void_p(self._K.data_ptr()), C.c_void_p(a[0].data_ptr()),
+                                         C.c_void_p(a[1].data_ptr()), C.c_void_p(b[0].data_ptr()),
+                                         C.c_void_p(b[1].data_ptr()), C.c_void_p(seg.data_ptr()),
+                                         C.c_void_p(self._gK.data_ptr()), m, self.steps_per_pass,
+                                         C.c_void_p(self._work.data_ptr()), C.byref(self.grid),
+                                         C.c_void_p(stream_ptr(self._K))), "pde_wave_adjoint")
+            a, b = b, a
+        torch.sub(a[0], a[1], out=self._gu)  # dJ/du0 = mu^0 + mu^{-1} = mu^0 - mu^1
+
+    # -- public ------------------------------------------------------------------
     def forward(self, K: torch.Tensor, u0: torch.Tensor) -> torch.Tensor:
-        """u^N from u^{-1} = u^0 = u0; keeps (u^{n-1}, u^n) at n = 0, every, 2*every, ..."""
+        """u^N from u^{-1} = u^0 = u0 (restricted to the cells inside the node ring)."""
         require_cuda_f32(K, "K")
         require_cuda_f32(u0, "u0")
         self._buffers(K)
-        self.checkpoints = []
-        u0 = u0 * interior_mask(self.shape, self.g, u0.device)  # the state lives inside the node ring
-        prev, cur = u0.clone(), u0.clone()
-        n = 0
-        self._last_seg_ready = False
-        while n < self.N:
-            self.checkpoints.append((n, prev.clone(), cur.clone()))
-            m = min(self.every, self.N - n)
-            op, oc = torch.empty_like(cur), torch.empty_like(cur)
-            if n + m == self.N:
-                # the last segment keeps its states: the adjoint starts there without recomputing
-                self._seg[0].copy_(cur.reshape(-1))
-                self._fwd(K, prev, cur, op, oc, n, m, states=self._seg[1:m + 1])
-                self._last_seg_ready = True
-            else:
-                self._fwd(K, prev, cur, op, oc, n, m)
-            prev, cur, n = op, oc, n + m
-        return cur
+        self._K.copy_(K)
+        torch.mul(u0, self._mask, out=self._u0)  # the state lives inside the node ring
+        self._seq_f.run()
+        self._fwd_done = True
+        return self._out[1].clone()
 
     def backward(self, K: torch.Tensor, dJ_duN: torch.Tensor):
         """(dJ/dK, dJ/du0) for the last forward()."""
-        self._buffers(K)
-        gK = torch.zeros_like(K)
-        mu1, mu2 = dJ_duN.contiguous().clone(), torch.zeros_like(dJ_duN)
-        kept = self._last_seg_ready
-        self._last_seg_ready = False
-        for n0, prev, cur in reversed(self.checkpoints):
-            m = min(self.every, self.N - n0)
-            seg = self._seg[: m]
-            if kept and n0 + m == self.N:
-                pass  # u^{n0} .. u^{N-1} were stored by forward()
-            else:
-                seg[0].copy_(cur.reshape(-1))
-                if m > 1:  # recompute u^{n0+1} .. u^{n0+m-1}
-                    op, oc = torch.empty_like(cur), torch.empty_like(cur)
-                    self._fwd(K, prev, cur, op, oc, n0, m - 1, states=seg[1:])
-            o1, o2 = torch.empty_like(mu1), torch.empty_like(mu2)
-            check(lib().pde_wave_adjoint(C.c_void_p(K.data_ptr()), C.c_void_p(mu1.data_ptr()),
-                                         C.c_void_p(mu2.data_ptr()), C.c_void_p(o1.data_ptr()),
-                                         C.c_void_p(o2.data_ptr()), C.c_void_p(seg.data_ptr()),
-                                         C.c_void_p(gK.data_ptr()), m, self.steps_per_pass,
-                                         C.c_void_p(self._work.data_ptr()), C.byref(self.grid),
-                                         C.c_void_p(stream_ptr(K))), "pde_wave_adjoint")
-            mu1, mu2 = o1, o2
-        return gK, mu1 - mu2  # dJ/du0 = mu^0 + mu^{-1} = mu^0 - mu^1
+        if not getattr(self, "_fwd_done", False):
+            raise RuntimeError("backward() needs a forward() first")
+        self._K.copy_(K)
+        self._g.copy_(dJ_duN)
+        self._seq_b.run()
+        return self._gK.clone(), self._gu.clone()
 
 
 class _WaveFn(torch.autograd.Function):
