@@ -390,8 +390,8 @@ def exchange_x_halos(f, g, rank, world):
     f[n - g:n].copy_(recv_hi)
 
 
-# output tiles tried for the temporally blocked 2D kernels ((0, 0): the library's automatic choice)
-TILES_2D = ((0, 0), (32, 64), (32, 32), (16, 32), (16, 64))
+# launch shapes (tile_x, tile_y, threads) tried for the temporally blocked 2D kernels (0: automatic)
+TILES_2D = ((0, 0, 0), (32, 64, 1024), (32, 64, 512), (32, 32, 512), (32, 32, 256), (16, 32, 256), (16, 64, 256))
 
 
 def run_heat(steps: int = 1000):
@@ -462,7 +462,7 @@ def run_heat(steps: int = 1000):
     import pde_module_b200._lib as L
     adj = {}
     for tile, k in [(t, q) for t in TILES_2D for q in (4, 8, 16)]:
-        L.check(L.lib().pde_set_tile_2d(*tile), "pde_set_tile_2d")
+        L.check(L.lib().pde_set_launch_2d(*tile), "pde_set_launch_2d")
         solver = P.HeatSolver(bc, dx, dt, steps, steps_per_pass=k)
         a_f = torch.ones_like(u0)
 
@@ -491,21 +491,21 @@ def run_heat(steps: int = 1000):
         f_ms, fa_ms = ev(fwd), ev(fwd_adj)
         adj[(tile, k)] = (f_ms, fa_ms)
     kb = min(adj, key=lambda q: adj[q][1])
-    L.check(L.lib().pde_set_tile_2d(*kb[0]), "pde_set_tile_2d")
+    L.check(L.lib().pde_set_launch_2d(*kb[0]), "pde_set_launch_2d")
     same_fwd = bool(torch.equal(P.HeatSolver(bc, dx, dt, steps, steps_per_pass=kb[1]).forward(torch.ones_like(u0),
                                                                                              u0), out_chain))
-    L.check(L.lib().pde_set_tile_2d(0, 0), "pde_set_tile_2d")
+    L.check(L.lib().pde_set_launch_2d(0, 0, 0), "pde_set_launch_2d")
     return {"workload": "2D heat 256^2, Dirichlet 0, 1000 steps (examples/2D_Heat_Equation.py loop)",
             "fused_cell_updates_per_s": cells / (best[0] / 1000.0), "fused_k": best[1],
             "chain_cell_updates_per_s": cells / (res["chain_ms"] / 1000.0),
             "speedup_vs_chain": res["chain_ms"] / best[0],
             "bitwise_equal_to_chain": bool(torch.equal(best[2], out_chain)),
             "times_ms": {k: round(v, 4) for k, v in res.items()},
-            "adjoint": {"steps_per_pass": kb[1], "tile": list(kb[0]) if kb[0] != (0, 0) else "auto",
+            "adjoint": {"steps_per_pass": kb[1], "launch": list(kb[0]) if kb[0] != (0, 0, 0) else "auto",
                         "forward_ms": adj[kb][0], "forward_adjoint_ms": adj[kb][1],
                         "ratio_fwd_adj_over_fwd": adj[kb][1] / adj[kb][0],
                         "forward_bitwise_equal_to_chain": same_fwd,
-                        "by_tile_k": {f"{q[0][0]}x{q[0][1]}_k{q[1]}": [round(v[0], 4), round(v[1], 4)]
+                        "by_launch_k": {f"{q[0][0]}x{q[0][1]}t{q[0][2]}_k{q[1]}": [round(v[0], 4), round(v[1], 4)]
                                       for q, v in adj.items()},
                         "note": "alpha as a field, grads w.r.t. alpha and u0, sqrt(N) checkpoints (every 32 "
                                 "steps), forward and backward each replayed as one CUDA graph"},
@@ -592,13 +592,13 @@ def run_wave(n: int = 512, steps: int = 2000):
     import pde_module_b200._lib as L
     best = None
     for tile in TILES_2D:
-        L.check(L.lib().pde_set_tile_2d(*tile), "pde_set_tile_2d")
+        L.check(L.lib().pde_set_launch_2d(*tile), "pde_set_launch_2d")
         for k in (4, 8, 12, 16):
             solver.steps_per_pass = k  # also drops the captured graphs
             ms, _ = timed(fwd_adj, 1)
             if best is None or ms < best[0]:
                 best = (ms, k, tile)
-    L.check(L.lib().pde_set_tile_2d(*best[2]), "pde_set_tile_2d")
+    L.check(L.lib().pde_set_launch_2d(*best[2]), "pde_set_launch_2d")
     solver.steps_per_pass = best[1]
     f_ms, _ = timed(fwd_only)
     fa_ms, (loss, gc, gu) = timed(fwd_adj)
@@ -608,7 +608,7 @@ def run_wave(n: int = 512, steps: int = 2000):
     fa_all_ms, (loss2, gc2, _) = timed(fwd_adj)
     solver.set_checkpoint_every(every)
     same = bool(torch.equal(gc, gc2))
-    L.check(L.lib().pde_set_tile_2d(0, 0), "pde_set_tile_2d")
+    L.check(L.lib().pde_set_launch_2d(0, 0, 0), "pde_set_launch_2d")
     cells = n * n * steps
     return {"workload": f"differentiable wave {n}^2, {steps} leapfrog steps, CFL 0.5, Ricker source, "
                         f"MSE vs target, grads w.r.t. speed and initial field, sqrt(N) checkpoints "
@@ -617,7 +617,7 @@ def run_wave(n: int = 512, steps: int = 2000):
             "store_all_states": {"forward_adjoint_ms": fa_all_ms, "ratio_fwd_adj_over_fwd": fa_all_ms / f_ms,
                                  "grad_bitwise_equal_to_checkpointed": same},
             "forward_cell_updates_per_s": cells / (f_ms / 1000.0), "steps_per_pass": best[1],
-            "tile": list(best[2]) if best[2] != (0, 0) else "auto",
+            "launch": list(best[2]) if best[2] != (0, 0, 0) else "auto",
             "loss": float(loss.item()), "grad_c_norm": float(gc.norm().item()),
             "grad_u0_norm": float(gu.norm().item())}
 
@@ -823,6 +823,8 @@ def run_profile_op(args):
     --iters timed calls.  --profile-op is lap2|lap4|grad2|grad4|div2|div4."""
     import torch
     import pde_module_b200 as P
+    if args.profile_op in ("wave", "heatadj", "batched"):
+        return run_profile_2d(args)
     op, order = args.profile_op[:-1], int(args.profile_op[-1])
     n = args.profile_n
     g = order // 2
@@ -850,6 +852,43 @@ def run_profile_op(args):
     ms = e0.elapsed_time(e1) / args.iters
     b = {"lap": 8, "grad": 16, "div": 16}[op]
     print(json.dumps({"profile_op": args.profile_op, "n": n, "ms": ms, "gbs": n ** 3 * b / ms / 1e6}))
+    return 0
+
+
+def run_profile_2d(args):
+    """The 2D time-stepping kernels for profilers, eager (no graphs), short runs:
+    wave    - 512^2 wave problem, 96 steps, forward + adjoint (k = 4, automatic tile)
+    heatadj - 256^2 heat, alpha field, 96 steps, forward + adjoint (k = 4)
+    batched - the 64-grid batched heat rollout, 16 steps (k = 4, 64 x 64 tiles)"""
+    import torch
+    import pde_module_b200 as P
+    from pde_module_b200.time_step import wave as W
+    t0 = time.time()
+    for _ in range(args.iters):
+        if args.profile_op == "wave":
+            solver, c, u0, target, dt, mask = W.make_problem(n=512, nsteps=96, steps_per_pass=4)
+            solver.graphs = False
+            solver.set_checkpoint_every(None)
+            K = (dt * dt) * c * c
+            uN = solver.forward(K, u0)
+            solver.backward(K, (uN - target) * mask)
+        elif args.profile_op == "heatadj":
+            n, g = 256, 1
+            dx = 1.0 / n
+            u0 = torch.rand((n + 2, n + 2, 1, 1), device="cuda")
+            bc = P.GridBoundary(u0, dx, g)
+            bc.dirichlet_BC("ALL", 0.0)
+            solver = P.HeatSolver(bc, dx, 0.2 * dx * dx, 96, steps_per_pass=4, graphs=False)
+            a = torch.ones_like(u0)
+            uN = solver.forward(a, u0)
+            solver.backward(a, uN)
+        else:
+            sides, alpha, u0, dx, dt = batched_problem()
+            fields = [torch.from_numpy(u[:, :, None, None]).cuda() for u in u0]
+            roll = P.BatchedHeatRollout(fields, dx, alpha, dt, tile=(64, 64), steps_per_pass=4)
+            roll(16)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_op": args.profile_op, "iters": args.iters, "s": round(time.time() - t0, 3)}))
     return 0
 
 

@@ -286,11 +286,13 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
 int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out,
                      float* mu_out_next, const float* lstates, float* grad_K, int32_t nsteps,
                      int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
-/* Output tile (cells) of the temporally blocked 2D kernels of pde_heat_forward,
- * pde_heat_adjoint, pde_wave_forward and pde_wave_adjoint, process-wide; (0, 0)
- * restores the automatic choice (the largest of 32x64, 32x32, 16x32 that gives
- * every SM a tile).  Sides 8..256. */
-int pde_set_tile_2d(int32_t tile_x, int32_t tile_y);
+/* Launch shape of the temporally blocked 2D kernels of pde_heat_forward,
+ * pde_heat_adjoint, pde_wave_forward and pde_wave_adjoint, process-wide:
+ * output tile (sides 8..256; (0, 0) = automatic: the largest of 32x64, 32x32,
+ * 16x32 that gives every SM a tile) and threads per block of the wave kernels
+ * (256, 512, 1024; 0 = automatic: 1024 with up to 1.1 tiles per SM, 512 up to
+ * 2.2, else 256; the heat kernels use 256). */
+int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads);
 
 /* ---- batched rollouts (new: the reference advances every grid with its own
  * module chain, examples/2D_Heat_Equation.py:57-65, three launches per step

@@ -129,84 +129,94 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
     const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, X);
     const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, Y);
     const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
-    // per-thread walk over the region (flattened, so every lane has a cell):
-    // start at cell tid, advance by blockDim.x = dq rows + dr cells
-    const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
-    const int lx_start = (int)threadIdx.x / RY, ly_start = (int)threadIdx.x - lx_start * RY;
-    float* A;  // buffer holding the newest level after the steps
+    const int OX = min(bx0 + P.TBX, X) - bx0, OY = min(by0 + P.TBY, Y) - by0;
+    const int nt = (int)blockDim.x;
+    // Each step walks its rectangle flattened (start at cell tid, advance by
+    // blockDim.x = dq rows + dr cells), so every lane has a cell.
     if (OP == BATCH_HEAT) {
-      A = sm;
+      // Both buffers start with the region; a step writes only its stencil
+      // rectangle, so cells outside it keep their loaded or last filled value.
+      float* A = sm;  // newest level
       float* B = sm + P.RC;
-      for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+      for (int i = threadIdx.x; i < RC; i += nt) {
         const int lx = i / RY, ly = i - lx * RY;
-        A[i] = in0[(size_t)(rx0 + lx) * Y + ry0 + ly];
+        const float* src = in0 + (size_t)(rx0 + lx) * Y + ry0 + ly;
+        cp_async4(A + i, src, true);
+        cp_async4(B + i, src, true);
       }
+      cp_async_wait_all();
       __syncthreads();
       H2Params HP;
       HP.X = X; HP.Y = Y; HP.g = g; HP.N = 1;
       const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
       const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
+      const int SW = max(sy1 - sy0, 1), SC = max(sx1 - sx0, 0) * max(sy1 - sy0, 0);
+      const int dq = nt / SW, dr = nt - dq * SW;
       for (int s = 0; s < ks; ++s) {
         bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, dx32);
-        int lx = lx_start, ly = ly_start;
-        for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+        int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
+        for (int c = threadIdx.x; c < SC; c += nt) {
+          const int i = (sx0 + lx) * RY + sy0 + ly;
           const float u2 = A[i];
-          float res = u2;
-          if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
-            float acc = 0.0f;
+          float acc = 0.0f;
 #pragma unroll
-            for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(w[t], A[i + (t - R) * RY]));
+          for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(w[t], A[i + (t - R) * RY]));
 #pragma unroll
-            for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(w[t], A[i + (t - R)]));
-            res = add(u2, mul(dt, mul(coef, acc)));
-          }
-          B[i] = res;
+          for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(w[t], A[i + (t - R)]));
+          B[i] = add(u2, mul(dt, mul(coef, acc)));
           lx += dq;
           ly += dr;
-          if (ly >= RY) { ly -= RY; ++lx; }
+          if (ly >= SW) { ly -= SW; ++lx; }
         }
         __syncthreads();
         float* t = A;
         A = B;
         B = t;
       }
+      // output: stencil cells from the newest level, the others as last filled (B)
+      for (int i = threadIdx.x; i < OX * OY; i += nt) {
+        const int lx = i / OY, ly = i - lx * OY;
+        const int x = bx0 + lx, y = by0 + ly;
+        const int ri = (x - rx0) * RY + (y - ry0);
+        const bool st = x >= g && x < X - g && y >= g && y < Y - g;
+        out0[(size_t)x * Y + y] = st ? A[ri] : B[ri];
+      }
     } else {
       float* Bm = sm;
       float* B0 = sm + P.RC;
       float* Bp = sm + 2 * P.RC;
-      // the state is zero outside the node ring (x, y in [g+1, n-g-2])
-      for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+      // the state is zero outside the node ring (x, y in [g+1, n-g-2]) in every buffer
+      for (int i = threadIdx.x; i < RC; i += nt) {
         const int lx = i / RY, ly = i - lx * RY;
         const int x = rx0 + lx, y = ry0 + ly;
         const bool inside = x > g && x < X - 1 - g && y > g && y < Y - 1 - g;
         const size_t gi = (size_t)x * Y + y;
-        Bm[i] = inside ? in1[gi] : 0.0f;
-        B0[i] = inside ? in0[gi] : 0.0f;
+        cp_async4(Bm + i, in1 + gi, inside);
+        cp_async4(B0 + i, in0 + gi, inside);
+        Bp[i] = 0.0f;
       }
+      cp_async_wait_all();
       __syncthreads();
+      // computed rectangle: inside the ring, one cell away from the region's edges
+      const int cx0 = max(g + 1, rx0 + 1) - rx0, cx1 = min(X - 1 - g, rx0 + RX - 1) - rx0;
+      const int cy0 = max(g + 1, ry0 + 1) - ry0, cy1 = min(Y - 1 - g, ry0 + RY - 1) - ry0;
+      const int CW = max(cy1 - cy0, 1), CC = max(cx1 - cx0, 0) * max(cy1 - cy0, 0);
+      const int dq = nt / CW, dr = nt - dq * CW;
       for (int s = 0; s < ks; ++s) {
-        int lx = lx_start, ly = ly_start;
-        for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-          const int x = rx0 + lx, y = ry0 + ly;
-          float v = 0.0f;
-          if (x > g && x < X - 1 - g && y > g && y < Y - 1 - g) {
-            if (lx >= 1 && lx < RX - 1 && ly >= 1 && ly < RY - 1) {
-              float acc = 0.0f;  // Laplacian, alpha 1 (FDM/kernel/laplacian.py:40-46 order)
-              acc = add(acc, mul(w[0], B0[i - RY]));
-              acc = add(acc, mul(w[1], B0[i]));
-              acc = add(acc, mul(w[2], B0[i + RY]));
-              acc = add(acc, mul(w[0], B0[i - 1]));
-              acc = add(acc, mul(w[1], B0[i]));
-              acc = add(acc, mul(w[2], B0[i + 1]));
-              v = add(sub(mul(2.0f, B0[i]), Bm[i]), mul(coef, acc));
-            } else {
-              v = B0[i];  // cut edge: not valid after this step, never output
-            }
-          }
-          Bp[i] = v;
+        int lx = (int)threadIdx.x / CW, ly = (int)threadIdx.x - lx * CW;
+        for (int c = threadIdx.x; c < CC; c += nt) {
+          const int i = (cx0 + lx) * RY + cy0 + ly;
+          float acc = 0.0f;  // Laplacian, alpha 1 (FDM/kernel/laplacian.py:40-46 order)
+          acc = add(acc, mul(w[0], B0[i - RY]));
+          acc = add(acc, mul(w[1], B0[i]));
+          acc = add(acc, mul(w[2], B0[i + RY]));
+          acc = add(acc, mul(w[0], B0[i - 1]));
+          acc = add(acc, mul(w[1], B0[i]));
+          acc = add(acc, mul(w[2], B0[i + 1]));
+          Bp[i] = add(sub(mul(2.0f, B0[i]), Bm[i]), mul(coef, acc));
           lx += dq;
           ly += dr;
-          if (ly >= RY) { ly -= RY; ++lx; }
+          if (ly >= CW) { ly -= CW; ++lx; }
         }
         __syncthreads();
         float* t = Bm;
@@ -214,17 +224,12 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
         B0 = Bp;
         Bp = t;
       }
-      A = B0;
-      const int OX = min(bx0 + P.TBX, X) - bx0, OY = min(by0 + P.TBY, Y) - by0;
-      for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
+      for (int i = threadIdx.x; i < OX * OY; i += nt) {
         const int lx = i / OY, ly = i - lx * OY;
-        out1[(size_t)(bx0 + lx) * Y + by0 + ly] = Bm[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+        const int ri = (bx0 + lx - rx0) * RY + (by0 + ly - ry0);
+        out1[(size_t)(bx0 + lx) * Y + by0 + ly] = Bm[ri];
+        out0[(size_t)(bx0 + lx) * Y + by0 + ly] = B0[ri];
       }
-    }
-    const int OX = min(bx0 + P.TBX, X) - bx0, OY = min(by0 + P.TBY, Y) - by0;
-    for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
-      const int lx = i / OY, ly = i - lx * OY;
-      out0[(size_t)(bx0 + lx) * Y + by0 + ly] = A[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
     }
     __threadfence();
     __syncthreads();

@@ -6,6 +6,17 @@
 
 namespace pde {
 
+// 4-byte asynchronous global -> shared copy (cp.async); src-size 0 writes a
+// zero instead of reading.  A thread's copies are all in flight at once, so a
+// region load costs one memory latency, not one per cell it copies.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+// Wait for this thread's cp.async copies (the block still needs a barrier before others read them).
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+
 // Geometry of one (X, Y, Z, N...) array, derived from PdeGrid.
 struct Geo {
   int64_t n[3];        // array extents including ghosts

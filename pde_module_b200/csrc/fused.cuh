@@ -231,7 +231,8 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
   // 2D thread layout: 32 lanes along the contiguous (y, component) floats, blockDim.x / 32 rows
   const int lf0 = threadIdx.x & 31, lx0 = threadIdx.x >> 5, nrows = blockDim.x >> 5;
   for (int lx = lx0; lx < RX; lx += nrows)
-    for (int lf = lf0; lf < nrow; lf += 32) A[lx * nrow + lf] = __ldg(in + ((size_t)(rx0 + lx) * P.Y + ry0) * N + lf);
+    for (int lf = lf0; lf < nrow; lf += 32) cp_async4(A + lx * nrow + lf, in + ((size_t)(rx0 + lx) * P.Y + ry0) * N + lf, true);
+  cp_async_wait_all();
   __syncthreads();
   const int g = P.g;
   // stencil cells whose R neighbours along both axes are inside the region

@@ -67,9 +67,10 @@ __global__ void __launch_bounds__(256) heat2d_field_fwd_kernel(const float* __re
   for (int i = threadIdx.x; i < RC; i += blockDim.x) {
     const int lx = i / RY, ly = i - lx * RY;
     const size_t gi = (size_t)(rx0 + lx) * Y + ry0 + ly;
-    A[i] = __ldg(in + gi);
-    AL[i] = __ldg(P.alpha + gi);
+    cp_async4(A + i, in + gi, true);
+    cp_async4(AL + i, P.alpha + gi, true);
   }
+  cp_async_wait_all();
   __syncthreads();
   H2Params HP;
   HP.X = X; HP.Y = Y; HP.g = g; HP.N = 1;
@@ -167,16 +168,18 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
   const float dt = P.dt;
   for (int i = threadIdx.x; i < RC; i += blockDim.x) {
     const int lx = i / RY, ly = i - lx * RY;
-    const int x = rx0 + lx, y = ry0 + ly;
-    const size_t gi = (size_t)x * Y + y;
-    const float l = __ldg(lam_in + gi), a = __ldg(P.alpha + gi);
-    Lm[i] = l;
-    AL[i] = a;
-    Z[i] = heat_stencil_cell(x, y, X, Y, g) ? mul(dt, mul(a, l)) : 0.0f;
+    const size_t gi = (size_t)(rx0 + lx) * Y + ry0 + ly;
+    cp_async4(Lm + i, lam_in + gi, true);
+    cp_async4(AL + i, P.alpha + gi, true);
   }
   for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
     const int lx = i / OY, ly = i - lx * OY;
-    GA[i] = P.galpha[(size_t)(bx0 + lx) * Y + by0 + ly];
+    cp_async4(GA + i, P.galpha + (size_t)(bx0 + lx) * Y + by0 + ly, true);
+  }
+  cp_async_wait_all();
+  for (int i = threadIdx.x; i < RC; i += blockDim.x) {  // the cells this thread copied
+    const int lx = i / RY, ly = i - lx * RY;
+    Z[i] = heat_stencil_cell(rx0 + lx, ry0 + ly, X, Y, g) ? mul(dt, mul(AL[i], Lm[i])) : 0.0f;
   }
   __syncthreads();
   const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;

@@ -539,8 +539,19 @@ namespace {
 
 // Output tile of the temporally blocked 2D kernels (differentiable heat, wave):
 // the largest of 32x64, 32x32, 16x32 that still gives every SM a tile, unless
-// pde_set_tile_2d fixed one.
+// pde_set_launch_2d fixed one.
 int g_tile2d[2] = {0, 0};
+int g_threads2d = 0;
+
+// Threads per block for the wave kernels: enough warps per SM to hide shared-
+// memory latency when tiles are few (up to 1024), 256 when every SM has several.
+int pick_threads_2d(long long tiles) {
+  if (g_threads2d > 0) return g_threads2d;
+  const double per_sm = (double)tiles / sm_count();
+  if (per_sm <= 1.1) return 1024;
+  if (per_sm <= 2.2) return 512;
+  return 256;
+}
 
 void pick_tile_2d(int X, int Y, int* tbx, int* tby) {
   if (g_tile2d[0] > 0) {
@@ -588,14 +599,13 @@ int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_
 
 extern "C" {
 
-int pde_set_tile_2d(int32_t tile_x, int32_t tile_y) {
-  if (tile_x == 0 && tile_y == 0) {
-    g_tile2d[0] = g_tile2d[1] = 0;
-    return PDE_OK;
-  }
-  if (tile_x < 8 || tile_y < 8 || tile_x > 256 || tile_y > 256) return PDE_ERR_ARG;
+int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads) {
+  if (threads != 0 && threads != 256 && threads != 512 && threads != 1024) return PDE_ERR_ARG;
+  if (!(tile_x == 0 && tile_y == 0) && (tile_x < 8 || tile_y < 8 || tile_x > 256 || tile_y > 256))
+    return PDE_ERR_ARG;
   g_tile2d[0] = tile_x;
   g_tile2d[1] = tile_y;
+  g_threads2d = threads;
   return PDE_OK;
 }
 
@@ -747,6 +757,7 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
   }
   PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_fwd_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  const int threads = pick_threads_2d(tiles);
   const int npasses = (nsteps + k - 1) / k;
   float* w0 = work;
   float* w1 = work + P.cells;
@@ -761,7 +772,7 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
     P.lst = lstates ? lstates + (size_t)done * P.cells : nullptr;
     float* da = to_out ? out_prev : w0;
     float* db = to_out ? out_cur : w1;
-    wave_fwd_tb_kernel<<<tiles, 256, smem, st>>>(a, b, K, da, db, P);
+    wave_fwd_tb_kernel<<<tiles, threads, smem, st>>>(a, b, K, da, db, P);
     const int rc = launch_status();
     if (rc) return rc;
     a = da;
@@ -787,10 +798,12 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
   int k;
   size_t smem;
   if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 6, 1)) return PDE_ERR_UNSUPPORTED;
+
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)P.cells;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_adj_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  const int threads = pick_threads_2d(tiles);
   const int npasses = (nsteps + k - 1) / k;
   float* w0 = work;
   float* w1 = work + P.cells;
@@ -806,7 +819,7 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
     P.ntop = nsteps - 1 - done;
     float* da = to_out ? mu_out : w0;
     float* db = to_out ? mu_out_next : w1;
-    wave_adj_tb_kernel<<<tiles, 256, smem, st>>>(a, b, K, da, db, P);
+    wave_adj_tb_kernel<<<tiles, threads, smem, st>>>(a, b, K, da, db, P);
     const int rc = launch_status();
     if (rc) return rc;
     a = da;

@@ -11,7 +11,9 @@
 //
 // Both directions advance k steps per launch out of shared-memory tiles
 // (halo k cells; cells outside the node ring are constant zeros, so only the
-// region's cut edges lose one valid cell per step).  Every product and sum is
+// region's cut edges lose one valid cell per step).  Regions are loaded with
+// cp.async (every copy of a thread in flight at once; cells outside the ring
+// zero-filled), and each step computes only the rectangle of cells that change.  Every product and sum is
 // rounded on its own.  The forward can store L(u^n), the Laplacian it has just
 // formed, for the adjoint's gradient term; the adjoint keeps K o mu in shared
 // memory (each product formed once per cell and step, the same value every
@@ -21,6 +23,7 @@
 #include "common.cuh"
 
 namespace pde {
+
 
 struct WaveParams {
   int X, Y, g;
@@ -42,18 +45,6 @@ __device__ __forceinline__ bool wave_inside(const WaveParams& P, int x, int y) {
   return x > P.g && x < P.X - 1 - P.g && y > P.g && y < P.Y - 1 - P.g;
 }
 
-// Laplacian at region index i of a region with row length RY (alpha 1).
-__device__ __forceinline__ float lap5(const float* B, int i, int RY, const float* w) {
-  float acc = 0.0f;
-  acc = add(acc, mul(w[0], B[i - RY]));
-  acc = add(acc, mul(w[1], B[i]));
-  acc = add(acc, mul(w[2], B[i + RY]));
-  acc = add(acc, mul(w[0], B[i - 1]));
-  acc = add(acc, mul(w[1], B[i]));
-  acc = add(acc, mul(w[2], B[i + 1]));
-  return acc;
-}
-
 // Region of a tile: the tile grown by the halo H, clipped to the array.
 struct WaveRegion {
   int bx0, by0, rx0, ry0, RX, RY, OX, OY;
@@ -68,153 +59,194 @@ struct WaveRegion {
     OX = min(P.TBX, P.X - bx0);
     OY = min(P.TBY, P.Y - by0);
   }
-  __device__ int tile_to_region(int i) const {  // tile cell i (row-major OX x OY) -> region index
-    const int lx = i / OY, ly = i - lx * OY;
-    return (bx0 - rx0 + lx) * RY + (by0 - ry0 + ly);
-  }
-  __device__ size_t tile_to_global(int i, int Y) const {
-    const int lx = i / OY, ly = i - lx * OY;
-    return (size_t)(bx0 + lx) * Y + by0 + ly;
+};
+
+// Rectangle of region cells a step computes: inside the node ring and one cell
+// away from the region's edges (region indices [cx0, cx1) x [cy0, cy1)).  Cells
+// outside the ring hold 0 in every buffer; region-edge cells are never
+// rewritten, so their values go stale and, as cut edges do, invalidate one more
+// cell inward per step.  Tile cells inside the ring are at least k cells from
+// any cut edge, so they always lie in the rectangle.
+struct WaveRect {
+  int cx0, cy0, W, count;
+  __device__ WaveRect(const WaveParams& P, const WaveRegion& Rg) {
+    cx0 = max(P.g + 1, Rg.rx0 + 1) - Rg.rx0;
+    const int cx1 = min(P.X - 1 - P.g, Rg.rx0 + Rg.RX - 1) - Rg.rx0;
+    cy0 = max(P.g + 1, Rg.ry0 + 1) - Rg.ry0;
+    const int cy1 = min(P.Y - 1 - P.g, Rg.ry0 + Rg.RY - 1) - Rg.ry0;
+    W = max(cy1 - cy0, 0);
+    count = max(cx1 - cx0, 0) * W;
   }
 };
 
-__global__ void __launch_bounds__(256) wave_fwd_tb_kernel(const float* __restrict__ um_in,
-                                                           const float* __restrict__ u0_in,
-                                                           const float* __restrict__ Kf, float* __restrict__ um_out,
-                                                           float* __restrict__ u0_out, const WaveParams P) {
-  extern __shared__ __align__(16) float sm[];
-  const WaveRegion Rg(P, P.k);
-  const int RX = Rg.RX, RY = Rg.RY, RC = RX * RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
-  float* Bm = sm;
-  float* B0 = sm + P.RC;
-  float* Bp = sm + 2 * P.RC;
-  float* Kt = sm + 3 * P.RC;
-  for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-    const int lx = i / RY, ly = i - lx * RY;
-    const size_t gi = (size_t)(rx0 + lx) * P.Y + ry0 + ly;
-    const bool in = wave_inside(P, rx0 + lx, ry0 + ly);  // the state is zero outside the node ring
-    Bm[i] = in ? __ldg(um_in + gi) : 0.0f;
-    B0[i] = in ? __ldg(u0_in + gi) : 0.0f;
-    Kt[i] = __ldg(Kf + gi);
+// Walk of a row-major (rows x W) rectangle by a block: cell c = tid, tid + nt, ...
+// as (row, col), advanced without division.
+struct RectWalk {
+  int row, col, dq, dr, W;
+  __device__ RectWalk(int W_, int nt) : W(max(W_, 1)) {
+    dq = nt / W;
+    dr = nt - dq * W;
+    row = (int)threadIdx.x / W;
+    col = (int)threadIdx.x - row * W;
   }
-  __syncthreads();
-  const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
-  const int lxs = (int)threadIdx.x / RY, lys = (int)threadIdx.x - lxs * RY;
-  const int ox1 = Rg.bx0 + Rg.OX, oy1 = Rg.by0 + Rg.OY;
+  __device__ void next() {
+    row += dq;
+    col += dr;
+    if (col >= W) { col -= W; ++row; }
+  }
+};
+
+// Load a region row-major (RX x RY) with fn(region index, array x, array y).
+template <class F>
+__device__ __forceinline__ void for_region(const WaveRegion& Rg, F fn) {
+  RectWalk wk(Rg.RY, (int)blockDim.x);
+  for (int i = threadIdx.x; i < Rg.RX * Rg.RY; i += blockDim.x, wk.next()) fn(i, Rg.rx0 + wk.row, Rg.ry0 + wk.col);
+}
+
+// Tile cells (OX x OY) with fn(tile index, region index, global index).
+template <class F>
+__device__ __forceinline__ void for_tile(const WaveRegion& Rg, int Y, F fn) {
+  RectWalk wk(Rg.OY, (int)blockDim.x);
+  for (int t = threadIdx.x; t < Rg.OX * Rg.OY; t += blockDim.x, wk.next())
+    fn(t, (Rg.bx0 - Rg.rx0 + wk.row) * Rg.RY + (Rg.by0 - Rg.ry0 + wk.col),
+       (size_t)(Rg.bx0 + wk.row) * Y + Rg.by0 + wk.col);
+}
+
+// Laplacian at shared-memory index i (alpha 1), rows of RY cells.
+__device__ __forceinline__ float lap5s(const float* sm, int i, int RY, const float* w) {
+  float acc = 0.0f;
+  acc = add(acc, mul(w[0], sm[i - RY]));
+  acc = add(acc, mul(w[1], sm[i]));
+  acc = add(acc, mul(w[2], sm[i + RY]));
+  acc = add(acc, mul(w[0], sm[i - 1]));
+  acc = add(acc, mul(w[1], sm[i]));
+  acc = add(acc, mul(w[2], sm[i + 1]));
+  return acc;
+}
+
+// k forward steps; the three levels are rotated as offsets into the one
+// shared-memory array (om: u^{n-1}, o0: u^n, op: u^{n+1}).
+template <bool STORE>
+__device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRegion& Rg, float* sm, int& om,
+                                               int& o0, int& op, int ok) {
+  const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
+  const WaveRect Rt(P, Rg);
+  const int nt = (int)blockDim.x;
+  const int srci = (P.srcx >= 0 && P.srcx >= rx0 && P.srcx < rx0 + Rg.RX && P.srcy >= ry0 && P.srcy < ry0 + RY)
+                       ? (P.srcx - rx0) * RY + (P.srcy - ry0) : -1;
+  // the tile in rectangle coordinates (for the stored Laplacians)
+  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
   for (int s = 0; s < P.k; ++s) {
-    const float sn = (P.srcx >= 0) ? P.src[P.n0 + s] : 0.0f;
-    float* Ls = P.lst ? P.lst + (size_t)s * P.cells : nullptr;
-    int lx = lxs, ly = lys;
-    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-      const int x = rx0 + lx, y = ry0 + ly;
-      float v = 0.0f, lap = 0.0f;
-      if (wave_inside(P, x, y)) {
-        if (lx >= 1 && lx < RX - 1 && ly >= 1 && ly < RY - 1) {
-          lap = lap5(B0, i, RY, P.w);
-          v = sub(mul(2.0f, B0[i]), Bm[i]);
-          v = add(v, mul(Kt[i], lap));
-          if (x == P.srcx && y == P.srcy) v = add(v, sn);
-        } else {
-          v = B0[i];  // cut edge: not valid after this step, never output
-        }
+    const float sn = (srci >= 0) ? P.src[P.n0 + s] : 0.0f;
+    float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
+    RectWalk wk(Rt.W, nt);
+    for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
+      const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
+      const float lap = lap5s(sm, o0 + i, RY, P.w);
+      float v = sub(mul(2.0f, sm[o0 + i]), sm[om + i]);
+      v = add(v, mul(sm[ok + i], lap));
+      if (i == srci) v = add(v, sn);
+      sm[op + i] = v;
+      if (STORE) {
+        const int ox = wk.row - tx0, oy = wk.col - ty0;
+        if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY)
+          Ls[(size_t)(Rg.bx0 + ox) * P.Y + Rg.by0 + oy] = lap;
       }
-      Bp[i] = v;
-      if (Ls && x >= Rg.bx0 && x < ox1 && y >= Rg.by0 && y < oy1) Ls[(size_t)x * P.Y + y] = lap;
-      lx += dq;
-      ly += dr;
-      if (ly >= RY) { ly -= RY; ++lx; }
     }
     __syncthreads();
-    float* t = Bm;
-    Bm = B0;
-    B0 = Bp;
-    Bp = t;
-  }
-  for (int i = threadIdx.x; i < Rg.OX * Rg.OY; i += blockDim.x) {
-    const size_t gi = Rg.tile_to_global(i, P.Y);
-    const int ri = Rg.tile_to_region(i);
-    um_out[gi] = Bm[ri];
-    u0_out[gi] = B0[ri];
+    const int t = om;
+    om = o0;
+    o0 = op;
+    op = t;
   }
 }
 
-__global__ void __launch_bounds__(256) wave_adj_tb_kernel(const float* __restrict__ m1_in,
-                                                           const float* __restrict__ m2_in,
-                                                           const float* __restrict__ Kf, float* __restrict__ m1_out,
-                                                           float* __restrict__ m2_out, const WaveParams P) {
+__global__ void __launch_bounds__(1024) wave_fwd_tb_kernel(const float* __restrict__ um_in,
+                                                            const float* __restrict__ u0_in,
+                                                            const float* __restrict__ Kf, float* __restrict__ um_out,
+                                                            float* __restrict__ u0_out, const WaveParams P) {
   extern __shared__ __align__(16) float sm[];
   const WaveRegion Rg(P, P.k);
-  const int RX = Rg.RX, RY = Rg.RY, RC = RX * RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
-  float* M2 = sm;
-  float* M1 = sm + P.RC;
-  float* M0 = sm + 2 * P.RC;
-  float* KM1 = sm + 3 * P.RC;  // K o mu^{n+1}
-  float* KM0 = sm + 4 * P.RC;  // K o mu^{n}, formed with mu^n
-  float* Kt = sm + 5 * P.RC;
-  float* GA = sm + 6 * P.RC;   // dJ/dK of the tile (OX x OY)
-  for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-    const int lx = i / RY, ly = i - lx * RY;
-    const size_t gi = (size_t)(rx0 + lx) * P.Y + ry0 + ly;
-    const bool in = wave_inside(P, rx0 + lx, ry0 + ly);
-    const float m1 = in ? __ldg(m1_in + gi) : 0.0f, kk = __ldg(Kf + gi);
-    M2[i] = in ? __ldg(m2_in + gi) : 0.0f;
-    M1[i] = m1;
-    Kt[i] = kk;
-    KM1[i] = mul(kk, m1);
-  }
-  for (int i = threadIdx.x; i < Rg.OX * Rg.OY; i += blockDim.x) GA[i] = P.gK[Rg.tile_to_global(i, P.Y)];
+  int om = 0, o0 = P.RC, op = 2 * P.RC;
+  const int ok = 3 * P.RC;
+  for_region(Rg, [&](int i, int x, int y) {
+    const size_t gi = (size_t)x * P.Y + y;
+    const bool in = wave_inside(P, x, y);  // the state is zero outside the node ring
+    cp_async4(sm + om + i, um_in + gi, in);
+    cp_async4(sm + o0 + i, u0_in + gi, in);
+    cp_async4(sm + ok + i, Kf + gi, true);
+    sm[op + i] = 0.0f;
+  });
+  cp_async_wait_all();
   __syncthreads();
-  const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
-  const int lxs = (int)threadIdx.x / RY, lys = (int)threadIdx.x - lxs * RY;
-  const int ox1 = Rg.bx0 + Rg.OX, oy1 = Rg.by0 + Rg.OY;
+  if (P.lst) wave_fwd_steps<true>(P, Rg, sm, om, o0, op, ok);
+  else wave_fwd_steps<false>(P, Rg, sm, om, o0, op, ok);
+  for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
+    um_out[gi] = sm[om + ri];
+    u0_out[gi] = sm[o0 + ri];
+  });
+}
+
+__global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restrict__ m1_in,
+                                                            const float* __restrict__ m2_in,
+                                                            const float* __restrict__ Kf, float* __restrict__ m1_out,
+                                                            float* __restrict__ m2_out, const WaveParams P) {
+  extern __shared__ __align__(16) float sm[];
+  const WaveRegion Rg(P, P.k);
+  const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
+  // offsets into sm: mu^{n+2}, mu^{n+1}, mu^n; K o mu^{n+1}, K o mu^n; K; dJ/dK of the tile
+  int o2 = 0, o1 = P.RC, o0 = 2 * P.RC, k1 = 3 * P.RC, k0 = 4 * P.RC;
+  const int okk = 5 * P.RC, oga = 6 * P.RC;
+  for_region(Rg, [&](int i, int x, int y) {
+    const size_t gi = (size_t)x * P.Y + y;
+    const bool in = wave_inside(P, x, y);
+    cp_async4(sm + o2 + i, m2_in + gi, in);
+    cp_async4(sm + o1 + i, m1_in + gi, in);
+    cp_async4(sm + okk + i, Kf + gi, true);
+    sm[o0 + i] = 0.0f;
+    sm[k0 + i] = 0.0f;
+  });
+  for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, P.gK + gi, true); });
+  cp_async_wait_all();
+  // K o mu^{n+1} of the cells this thread copied (its own copies are complete)
+  for_region(Rg, [&](int i, int x, int y) { sm[k1 + i] = mul(sm[okk + i], sm[o1 + i]); });
+  __syncthreads();
+  const WaveRect Rt(P, Rg);
+  const int nt = (int)blockDim.x;
+  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
   for (int s = 0; s < P.k; ++s) {
     const float* Ln = P.lsts + (size_t)(P.ntop - s) * P.cells;
-    int lx = lxs, ly = lys;
-    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-      const int x = rx0 + lx, y = ry0 + ly;
-      float v = 0.0f;
-      if (wave_inside(P, x, y)) {
-        if (lx >= 1 && lx < RX - 1 && ly >= 1 && ly < RY - 1) {
-          // L(K o mu^{n+1})
-          float acc = 0.0f;
-          acc = add(acc, mul(P.w[0], KM1[i - RY]));
-          acc = add(acc, mul(P.w[1], KM1[i]));
-          acc = add(acc, mul(P.w[2], KM1[i + RY]));
-          acc = add(acc, mul(P.w[0], KM1[i - 1]));
-          acc = add(acc, mul(P.w[1], KM1[i]));
-          acc = add(acc, mul(P.w[2], KM1[i + 1]));
-          v = add(sub(mul(2.0f, M1[i]), M2[i]), acc);
-        } else {
-          v = M1[i];
-        }
-        // gradient term of step n on the tile: dJ/dK += mu^{n+1} o L(u^n)
-        if (x >= Rg.bx0 && x < ox1 && y >= Rg.by0 && y < oy1) {
-          const int t = (x - Rg.bx0) * Rg.OY + (y - Rg.by0);
-          GA[t] = add(GA[t], mul(M1[i], __ldg(Ln + (size_t)x * P.Y + y)));
+    RectWalk wk(Rt.W, nt);
+    for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
+      const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
+      const float m1 = sm[o1 + i];
+      {  // gradient term of step n on the tile: dJ/dK += mu^{n+1} o L(u^n)
+        const int ox = wk.row - tx0, oy = wk.col - ty0;
+        if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) {
+          const int t = oga + ox * Rg.OY + oy;
+          sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * P.Y + Rg.by0 + oy)));
         }
       }
-      M0[i] = v;
-      KM0[i] = mul(Kt[i], v);
-      lx += dq;
-      ly += dr;
-      if (ly >= RY) { ly -= RY; ++lx; }
+      // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+      const float acc = lap5s(sm, k1 + i, RY, P.w);
+      const float v = add(sub(mul(2.0f, m1), sm[o2 + i]), acc);
+      sm[o0 + i] = v;
+      sm[k0 + i] = mul(sm[okk + i], v);
     }
     __syncthreads();
-    float* t = M2;
-    M2 = M1;
-    M1 = M0;
-    M0 = t;
-    t = KM1;
-    KM1 = KM0;
-    KM0 = t;
+    const int t = o2;
+    o2 = o1;
+    o1 = o0;
+    o0 = t;
+    const int u = k1;
+    k1 = k0;
+    k0 = u;
   }
-  for (int i = threadIdx.x; i < Rg.OX * Rg.OY; i += blockDim.x) {
-    const size_t gi = Rg.tile_to_global(i, P.Y);
-    const int ri = Rg.tile_to_region(i);
-    m1_out[gi] = M1[ri];
-    m2_out[gi] = M2[ri];
-    P.gK[gi] = GA[i];
-  }
+  for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
+    m1_out[gi] = sm[o1 + ri];
+    m2_out[gi] = sm[o2 + ri];
+    P.gK[gi] = sm[oga + t];
+  });
 }
 
 }  // namespace pde

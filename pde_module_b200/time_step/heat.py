@@ -107,7 +107,10 @@ class HeatSolver:
         cells = self.shape[0] * self.shape[1]
         z = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)
         self._work = z(cells)
+        self._work_r = z(cells)  # the recomputation's own scratch
         self._seg = z(max(self.every, 1), cells)
+        self._seg2 = z(max(self.every, 1), cells) if len(self.segments) > 1 else self._seg
+        self._side = torch.cuda.Stream(device=dev)
         self._alpha, self._g = z(*f), z(*f)
         self._ck = z(max(len(self.segments), 1), *f)  # u^{n0} per segment
         self._out = z(*f)
@@ -118,9 +121,10 @@ class HeatSolver:
         self._seq_f.reset()
         self._seq_b.reset()
 
-    def _fwd(self, alpha, u, out, nsteps, lstates=None):
+    def _fwd(self, alpha, u, out, nsteps, lstates=None, work=None):
+        work = self._work if work is None else work
         check(lib().pde_heat_forward(C.c_void_p(alpha.data_ptr()), C.c_void_p(u.data_ptr()),
-                                     C.c_void_p(out.data_ptr()), C.c_void_p(self._work.data_ptr()),
+                                     C.c_void_p(out.data_ptr()), C.c_void_p(work.data_ptr()),
                                      C.byref(self.grid), C.byref(self.rules), self.dt, int(nsteps),
                                      self.steps_per_pass,
                                      C.c_void_p(lstates.data_ptr()) if lstates is not None else None,
@@ -141,20 +145,40 @@ class HeatSolver:
             self._out.copy_(self._ck[0])
 
     def _run_backward(self) -> None:
+        """Segments from the last to the first.  The adjoint of segment j (this
+        stream) runs while a second stream recomputes S of segment j-1 into the
+        other of two buffers; events order each buffer's reuse."""
+        main, side = torch.cuda.current_stream(), self._side
+        J = len(self.segments) - 1
+        bufs = (self._seg, self._seg2)  # segment j uses bufs[(J - j) % 2]; the forward filled bufs[0]
         self._ga.zero_()
         a, b = self._lam[0], self._lam[1]
         a.copy_(self._g)
-        for j in range(len(self.segments) - 1, -1, -1):
+        side.wait_stream(main)
+        rec_done, adj_done = {}, {}
+        for j in range(J, -1, -1):
+            if j >= 1:  # recompute S^{n0} .. S^{n0+m-1} of segment j-1 from its checkpoint
+                n0, m = self.segments[j - 1]
+                with torch.cuda.stream(side):
+                    if j + 1 in adj_done:
+                        side.wait_event(adj_done[j + 1])  # its buffer was segment j+1's
+                    self._fwd(self._alpha, self._ck[j - 1], self._tmp, m, bufs[(J - j + 1) % 2][:m],
+                              work=self._work_r)
+                    rec_done[j - 1] = torch.cuda.Event()
+                    rec_done[j - 1].record(side)
             n0, m = self.segments[j]
-            seg = self._seg[:m]
-            if j != len(self.segments) - 1:  # recompute S^{n0} .. S^{n0+m-1} from the checkpoint
-                self._fwd(self._alpha, self._ck[j], self._tmp, m, seg)
+            if j in rec_done:
+                main.wait_event(rec_done[j])
+            seg = bufs[(J - j) % 2][:m]
             check(lib().pde_heat_adjoint(C.c_void_p(self._alpha.data_ptr()), C.c_void_p(a.data_ptr()),
                                          C.c_void_p(b.data_ptr()), C.c_void_p(seg.data_ptr()),
                                          C.c_void_p(self._ga.data_ptr()), C.byref(self.grid), C.byref(self.rules),
                                          self.dt, m, self.steps_per_pass, C.c_void_p(self._work.data_ptr()),
-                                         C.c_void_p(stream_ptr(a))), "pde_heat_adjoint")
+                                         C.c_void_p(main.cuda_stream)), "pde_heat_adjoint")
+            adj_done[j] = torch.cuda.Event()
+            adj_done[j].record(main)
             a, b = b, a
+        main.wait_stream(side)
 
     def forward(self, alpha: torch.Tensor, u0: torch.Tensor) -> torch.Tensor:
         """u^N for diffusivity field alpha and initial field u0."""

@@ -98,3 +98,20 @@ def test_scalar_alpha_gradient_by_broadcast():
         um = solver.forward(torch.full((34, 34, 1, 1), 0.9 - eps, device="cuda"), u).double().sum()
     fd = float((up - um) / (2 * eps))
     assert abs(float(s.grad) - fd) <= 5e-3 * abs(fd)
+
+
+def test_graph_replay_with_solvers_replaced_in_a_loop():
+    """Solvers rebuilt in a loop (as a tuning sweep does) each capture and replay
+    their graphs; dropped solvers are freed outside any capture."""
+    groups, g, order, dx, dt, alpha, u0, lamN, bc = _setup("mixed", 48, 80, 40)
+    a0, u = torch.from_numpy(alpha).cuda(), torch.from_numpy(u0).cuda()
+    ref = None
+    for k in (2, 4, 8, 2, 4, 8):
+        solver = HeatSolver(bc, dx, dt, 40, steps_per_pass=k)
+        for _ in range(2):
+            a = a0.clone().requires_grad_(True)
+            loss = (heat_rollout(a, u, solver) ** 2).mean()
+            loss.backward()
+            if ref is None:
+                ref = a.grad.clone()
+            assert torch.equal(a.grad, ref)
