@@ -165,6 +165,17 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
   float* M = sm + 2 * P.RC;
   float* AL = sm + 3 * P.RC;
   float* GA = sm + 4 * P.RC;  // dJ/dalpha of the tile (OX x OY)
+  // S^n of the tile for the current and the next step (two slots): the next
+  // step's values are copied in (cp.async) while the current step computes
+  float* GL = GA + P.TBX * P.TBY;
+  const int OT = OX * OY;
+  auto fetch_S = [&](int s, int slot) {
+    const float* Sn = P.lsts + (size_t)(P.ntop - s) * P.cells;
+    for (int i = threadIdx.x; i < OT; i += blockDim.x) {
+      const int lx = i / OY, ly = i - lx * OY;
+      cp_async4(GL + slot * OT + i, Sn + (size_t)(bx0 + lx) * Y + by0 + ly, true);
+    }
+  };
   const float dt = P.dt;
   for (int i = threadIdx.x; i < RC; i += blockDim.x) {
     const int lx = i / RY, ly = i - lx * RY;
@@ -176,6 +187,7 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
     const int lx = i / OY, ly = i - lx * OY;
     cp_async4(GA + i, P.galpha + (size_t)(bx0 + lx) * Y + by0 + ly, true);
   }
+  fetch_S(0, 0);
   cp_async_wait_all();
   for (int i = threadIdx.x; i < RC; i += blockDim.x) {  // the cells this thread copied
     const int lx = i / RY, ly = i - lx * RY;
@@ -185,7 +197,8 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
   const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
   const int lxs = (int)threadIdx.x / RY, lys = (int)threadIdx.x - lxs * RY;
   for (int s = 0; s < P.k; ++s) {
-    const float* Sn = P.lsts + (size_t)(P.ntop - s) * P.cells;
+    if (s + 1 < P.k) fetch_S(s + 1, (s + 1) & 1);  // its slot was last read in step s-1
+    const float* Sg = GL + (s & 1) * OT;
     // mu = lam + L^T(z); the gradient term of step n on the tile
     int lx = lxs, ly = lys;
     for (int i = threadIdx.x; i < RC; i += blockDim.x) {
@@ -207,7 +220,7 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
       const int x = rx0 + lx, y = ry0 + ly;
       if (x >= bx0 && x < ox1 && y >= by0 && y < oy1 && heat_stencil_cell(x, y, X, Y, g)) {
         const int gi = (x - bx0) * OY + (y - by0);
-        GA[gi] = add(GA[gi], mul(l, mul(dt, __ldg(Sn + (size_t)x * Y + y))));
+        GA[gi] = add(GA[gi], mul(l, mul(dt, Sg[gi])));
       }
       lx += dq;
       ly += dr;
@@ -232,6 +245,7 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
       ly += dr;
       if (ly >= RY) { ly -= RY; ++lx; }
     }
+    cp_async_wait_all();  // this thread's copies of the next step's S; the barrier publishes them
     __syncthreads();
   }
   for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
