@@ -113,9 +113,10 @@ class ClockSampler:
 
 
 # ------------------------------------------------------- CPU baseline ---
-def cpu_sweep_sample(n: int, threads: int, reps: int = 1):
+def cpu_sweep_sample(n: int, threads: int, reps: int = 1, min_seconds: float = 0.0):
     """Time the float32 oracle over the 6-operator step on an n^3 interior,
-    split into X slabs over `threads` threads (NumPy releases the GIL)."""
+    split into X slabs over `threads` threads (NumPy releases the GIL); at least
+    `reps` repetitions and at least `min_seconds` of work."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import fdm
     rng = np.random.default_rng(1)
@@ -137,8 +138,10 @@ def cpu_sweep_sample(n: int, threads: int, reps: int = 1):
 
     bounds = np.linspace(0, n, threads + 1).astype(int)
     t0 = time.perf_counter()
+    done = 0
     with ThreadPoolExecutor(threads) as ex:
-        for _ in range(reps):
+        while done < reps or time.perf_counter() - t0 < min_seconds:
+            done += 1
             futs = []
             for order in (2, 4):
                 g = order // 2
@@ -148,7 +151,15 @@ def cpu_sweep_sample(n: int, threads: int, reps: int = 1):
             for f in futs:
                 f.result()
     dt = time.perf_counter() - t0
-    return 6 * n ** 3 * reps / dt, dt
+    return 6 * n ** 3 * done / dt, dt
+
+
+def sweep_config(world: int) -> dict:
+    return {"workload": "3D operator sweep 512^3 (Laplacian, Grad, Divergence; order 2 and 4; periodic ghosts)",
+            "interior": [N_INT, N_INT, N_INT], "ops_per_step": 6,
+            "fields": "scalar (512+2g)^3 and vec3 (512+2g)^3 per order",
+            "l2": "inputs larger than L2 (>=543 MB each), no flush",
+            "parallelism": f"dp{world}" if world > 1 else "single"}
 
 
 def run_reference(args):
@@ -170,11 +181,11 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "3D operator sweep, bounded CPU sample", "interior": [n, n, n],
-                   "ops_per_step": 6, "orders": [2, 4]},
+        "config": sweep_config(args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"the 6-operator step on a {n}^3 interior (order 2 and 4), NumPy float32 "
-                                   f"restatement of the reference kernels, X slabs over {threads} threads"},
+                         "sample": f"each step: the 6-operator step on a {n}^3 interior (order 2 and 4), NumPy "
+                                   f"float32 restatement of the reference kernels (the reference's own code needs "
+                                   f"warp-lang, absent here), X slabs over {threads} threads; value per cell"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -197,6 +208,7 @@ def run_ours(args):
     import pde_module_b200 as P
     from pde_module_b200 import _lib
 
+    from pde_module_b200.distributed import exchange_slab_halos
     dx = 1.0 / N_INT
     fast_mods = {}
     gen = torch.Generator(device="cuda")
@@ -212,8 +224,8 @@ def run_ours(args):
             bc.periodic("ALL" if world == 1 else ("Y", "Z"))
             f.copy_(bc(f))
         if world > 1:
-            exchange_x_halos(u, g, rank, world)
-            exchange_x_halos(v, g, rank, world)
+            exchange_slab_halos(u, g)
+            exchange_slab_halos(v, g)
         mods = (P.Laplacian(1, dx, g, order=order), P.Grad(1, u.shape, dx, g, order=order),
                 P.Divergence(3, v.shape, dx, g, order=order))
         fast = (P.Laplacian(1, dx, g, order=order, fast=True), P.Grad(1, u.shape, dx, g, order=order, fast=True),
@@ -337,21 +349,17 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt = cpu_sweep_sample(96, threads)
+        v, dt = cpu_sweep_sample(128, threads, min_seconds=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"the 6-operator step on a 96^3 interior, NumPy float32 restatement of the reference "
-                         f"kernels (oracle/fdm.py), X slabs over {threads} threads, {dt:.2f} s"}
+               "sample": f"the 6-operator step on a 128^3 interior repeated for {dt:.1f} s, NumPy float32 "
+                         f"restatement of the reference kernels (oracle/fdm.py), X slabs over {threads} threads"}
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (standard normal, seeded)",
-            "config": {"workload": "3D operator sweep 512^3 (Laplacian, Grad, Divergence; order 2 and 4; "
-                                   "periodic ghosts)", "interior": [N_INT, N_INT, N_INT],
-                       "ops_per_step": len(ops), "fields": "scalar (512+2g)^3 and vec3 (512+2g)^3 per order",
-                       "l2": "inputs larger than L2 (>=543 MB each), no flush",
-                       "parallelism": f"dp{world}" if world > 1 else "single"},
+            "config": sweep_config(world),
             "roofline": roofline, "kernels": kern,
             "fast_mode": {"value": world * cells * len(ops) / (fast_ms_step / 1000.0), "unit": UNIT,
                           "kernels": kern_fast,
@@ -370,24 +378,6 @@ def run_ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
-
-
-def exchange_x_halos(f, g, rank, world):
-    """Periodic X ghost planes from the neighbouring ranks (once, before timing)."""
-    import torch
-    import torch.distributed as dist
-    left, right = (rank - 1) % world, (rank + 1) % world
-    n = f.shape[0]
-    send_lo = f[g:2 * g].contiguous()
-    send_hi = f[n - 2 * g:n - g].contiguous()
-    recv_lo = torch.empty_like(send_lo)
-    recv_hi = torch.empty_like(send_hi)
-    ops = [dist.P2POp(dist.isend, send_lo, left), dist.P2POp(dist.isend, send_hi, right),
-           dist.P2POp(dist.irecv, recv_hi, right), dist.P2POp(dist.irecv, recv_lo, left)]
-    for r in dist.batch_isend_irecv(ops):
-        r.wait()
-    f[0:g].copy_(recv_lo)
-    f[n - g:n].copy_(recv_hi)
 
 
 # launch shapes (tile_x, tile_y, threads) tried for the temporally blocked 2D kernels (0: automatic)
@@ -610,6 +600,7 @@ def run_wave(n: int = 512, steps: int = 2000):
     same = bool(torch.equal(gc, gc2))
     L.check(L.lib().pde_set_launch_2d(0, 0, 0), "pde_set_launch_2d")
     cells = n * n * steps
+    check = wave_gradient_check(solver, c, u0, target, dt, mask, gc, gu)
     return {"workload": f"differentiable wave {n}^2, {steps} leapfrog steps, CFL 0.5, Ricker source, "
                         f"MSE vs target, grads w.r.t. speed and initial field, sqrt(N) checkpoints "
                         f"(every {solver.every} steps)",
@@ -619,7 +610,54 @@ def run_wave(n: int = 512, steps: int = 2000):
             "forward_cell_updates_per_s": cells / (f_ms / 1000.0), "steps_per_pass": best[1],
             "launch": list(best[2]) if best[2] != (0, 0, 0) else "auto",
             "loss": float(loss.item()), "grad_c_norm": float(gc.norm().item()),
-            "grad_u0_norm": float(gu.norm().item())}
+            "grad_u0_norm": float(gu.norm().item()), "gradient_check": check}
+
+
+def wave_gradient_check(solver, c, u0, target, dt, mask, gc, gu, eps=1e-3):
+    """The full-size gradients against float64 torch autograd of the same leapfrog
+    model (weights unrounded, written here independently of the kernels) and a
+    float64 central difference J(c + eps d) - J(c - eps d) along a seeded direction d."""
+    import torch
+    X, Y = solver.shape[0], solver.shape[1]
+    dx = solver.dx
+    w0, w1 = 1.0 / (dx * dx), -2.0 / (dx * dx)
+    inside = mask[:, :, 0, 0].double()
+    src = solver.src.double()
+    sx, sy = divmod(solver.src_cell, Y)
+    tgt = target[:, :, 0, 0].double()
+
+    def J(c64, u064):
+        K = (dt * dt) * c64 * c64
+        u = u064 * inside
+        um = u
+        for k in range(solver.N):
+            lap = torch.zeros_like(u)
+            cc = u[1:-1, 1:-1]
+            lap[1:-1, 1:-1] = (w0 * u[:-2, 1:-1] + w1 * cc + w0 * u[2:, 1:-1]) + (
+                w0 * u[1:-1, :-2] + w1 * cc + w0 * u[1:-1, 2:])
+            v = 2.0 * u - um + K * lap
+            e = torch.zeros_like(v)
+            e[sx, sy] = src[k]
+            um, u = u, (v + e) * inside
+        return (((u - tgt) * inside) ** 2).sum() / inside.sum()
+
+    c64 = c[:, :, 0, 0].double().clone().requires_grad_(True)
+    u64 = u0[:, :, 0, 0].double().clone().requires_grad_(True)
+    loss64 = J(c64, u64)
+    loss64.backward()
+    g64, gu64 = c64.grad, u64.grad
+    g32, gu32 = gc[:, :, 0, 0].double(), gu[:, :, 0, 0].double()
+    d = torch.randn(X, Y, generator=torch.Generator(device=c.device).manual_seed(11), device=c.device,
+                    dtype=torch.float64) * inside
+    with torch.no_grad():
+        fd = float((J(c64 + eps * d, u64) - J(c64 - eps * d, u64)) / (2 * eps))
+    an64, an32 = float((g64 * d).sum()), float((g32 * d).sum())
+    rel = lambda a, b: float((a - b).norm() / b.norm()) if float(b.norm()) > 0 else None
+    return {"reference": "float64 torch autograd of the same model (GPU), and a float64 central difference",
+            "loss_float64": float(loss64.detach()), "rel_err_grad_c": rel(g32, g64), "rel_err_grad_u0": rel(gu32, gu64),
+            "fd_directional": fd, "adjoint_directional_float32": an32, "autograd_directional_float64": an64,
+            "rel_err_fd_vs_float64_autograd": abs(fd - an64) / abs(fd), "rel_err_fd_vs_adjoint": abs(fd - an32) / abs(fd),
+            "eps": eps}
 
 
 def batched_problem(n_grids: int = 64, lo: int = 64, hi: int = 1024):
