@@ -532,16 +532,24 @@ def run_ldc(steps: int = 2000, n: int = 1024):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    tune = {k: timed_rollout(k, 40) for k in (5, 10, 25)}
-    k = min(tune, key=tune.get)
+    import pde_module_b200._lib as L
+    tune = {}
+    for tile in ((0, 0), (32, 64), (64, 64), (48, 96), (32, 128)):
+        L.check(L.lib().pde_set_launch_2d(tile[0], tile[1], 0), "pde_set_launch_2d")
+        for kk in (5, 8, 10, 16):
+            tune[(tile, kk)] = timed_rollout(kk, 40)
+    tile, k = min(tune, key=tune.get)
+    L.check(L.lib().pde_set_launch_2d(tile[0], tile[1], 0), "pde_set_launch_2d")
     ms = timed_rollout(k, steps)
+    L.check(L.lib().pde_set_launch_2d(0, 0, 0), "pde_set_launch_2d")
     u = s.u.cpu().numpy()
     cells = n * n * steps
     return {"workload": f"lid-driven cavity Re 100, {n}^2 nodes, fractional step, 50 Jacobi sweeps/step, "
                         f"{steps} steps from rest, dt {s.dt:.3e}",
             "ms": ms, "cell_updates_per_s": cells / (ms / 1000.0),
             "jacobi_sweeps_per_s": 50 * steps / (ms / 1000.0), "jacobi_per_pass": k,
-            "tune_ms_40_steps": {str(kk): round(v, 3) for kk, v in tune.items()},
+            "jacobi_tile": list(tile) if tile != (0, 0) else "auto",
+            "tune_ms_40_steps": {f"{t[0]}x{t[1]}_k{kk}": round(v, 3) for (t, kk), v in tune.items()},
             "launches_per_step": 3 + -(-50 // k) + (1 if (-(-50 // k)) % 2 else 0),
             "max_abs_u": float(np.abs(u).max()),
             "note": "L2-resident (about 28 MB of fields); CUDA graph replay of the whole rollout"}
@@ -861,7 +869,7 @@ def run_profile_op(args):
     --iters timed calls.  --profile-op is lap2|lap4|grad2|grad4|div2|div4."""
     import torch
     import pde_module_b200 as P
-    if args.profile_op in ("wave", "heatadj", "batched"):
+    if args.profile_op in ("wave", "heatadj", "batched", "ldc"):
         return run_profile_2d(args)
     op, order = args.profile_op[:-1], int(args.profile_op[-1])
     n = args.profile_n
@@ -897,7 +905,8 @@ def run_profile_2d(args):
     """The 2D time-stepping kernels for profilers, eager (no graphs), short runs:
     wave    - 512^2 wave problem, 96 steps, forward + adjoint (k = 4, automatic tile)
     heatadj - 256^2 heat, alpha field, 96 steps, forward + adjoint (k = 4)
-    batched - the 64-grid batched heat rollout, 16 steps (k = 4, 64 x 64 tiles)"""
+    batched - the 64-grid batched heat rollout, 16 steps (k = 4, 64 x 64 tiles)
+    ldc     - the 1024^2 lid-driven cavity, 4 steps (50 Jacobi sweeps each)"""
     import torch
     import pde_module_b200 as P
     from pde_module_b200.time_step import wave as W
@@ -920,6 +929,9 @@ def run_profile_2d(args):
             a = torch.ones_like(u0)
             uN = solver.forward(a, u0)
             solver.backward(a, uN)
+        elif args.profile_op == "ldc":
+            s = P.FractionalStepLDC(n=1024, Re=100.0, jacobi_iters=50)
+            s.step(4)
         else:
             sides, alpha, u0, dx, dt = batched_problem()
             fields = [torch.from_numpy(u[:, :, None, None]).cuda() for u in u0]

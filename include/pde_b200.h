@@ -287,7 +287,8 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
                      float* mu_out_next, const float* lstates, float* grad_K, int32_t nsteps,
                      int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
 /* Launch shape of the temporally blocked 2D kernels of pde_heat_forward,
- * pde_heat_adjoint, pde_wave_forward and pde_wave_adjoint, process-wide:
+ * pde_heat_adjoint, pde_wave_forward, pde_wave_adjoint and the Jacobi sweeps of
+ * pde_ldc_rollout, process-wide:
  * output tile (sides 8..256; (0, 0) = automatic: the largest of 32x64, 32x32,
  * 16x32 that gives every SM a tile) and threads per block of the wave kernels
  * (256, 512, 1024; 0 = automatic: 1024 with up to 1.1 tiles per SM, 512 up to

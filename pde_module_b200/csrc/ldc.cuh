@@ -22,104 +22,144 @@ struct LdcConst {
   float nu, dt, inv_dt, h2;
 };
 
-// Predictor: thread per cell of the whole (X, Y, 1, 2) array.
+// The three pointwise kernels run one thread per cell on a 2D grid (row =
+// blockIdx.y).  A cell whose neighbours are all at least one cell inside the
+// node ring ("deep": x, y in [g+2, n-g-3]) reads raw values; the others go
+// through bc_eval2d, which returns the boundary-filled value of any cell.
+__device__ __forceinline__ bool ldc_deep(const Geo& G, int i, int j) {
+  return i >= G.g + 2 && i < (int)G.n[0] - G.g - 2 && j >= G.g + 2 && j < (int)G.n[1] - G.g - 2;
+}
+__device__ __forceinline__ bool ldc_stencil(const Geo& G, int i, int j) {
+  return i >= G.g && i < (int)G.n[0] - G.g && j >= G.g && j < (int)G.n[1] - G.g;
+}
+
+// Raw 2D access (ncomp N) with 32-bit cell indices.
+template <int N>
+struct Raw2 {
+  const float* u;
+  int n1;
+  __device__ __forceinline__ float operator()(int i, int j, int v) const { return __ldg(u + (i * n1 + j) * N + v); }
+};
+// Boundary-filled access.
+struct Bc2 {
+  const Geo& G;
+  const PdeBCRules& R;
+  const GlobalAcc& U;
+  __device__ __forceinline__ float operator()(int i, int j, int v) const { return bc_eval2d(G, R, U, i, j, v); }
+};
+
+// Predictor of one stencil cell: u* = u2 + dt * (nu*Lap(u2) - Grad(u2) u2), with u2 = BC_u(u).
+template <class Get>
+__device__ __forceinline__ void ldc_predict_cell(const Get& at, int i, int j, const LdcConst& K, float* res) {
+  const float uc[2] = {at(i, j, 0), at(i, j, 1)};
+  float nb[2][2][3];  // [axis][comp][tap]
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    nb[0][c][1] = uc[c];
+    nb[1][c][1] = uc[c];
+    nb[0][c][0] = at(i - 1, j, c);
+    nb[0][c][2] = at(i + 1, j, c);
+    nb[1][c][0] = at(i, j - 1, c);
+    nb[1][c][2] = at(i, j + 1, c);
+  }
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    float acc = 0.0f;  // Laplacian, FDM/kernel/laplacian.py:40-46 order
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int t = 0; t < 3; ++t) acc = add(acc, mul(K.wl[t], nb[a][c][t]));
+    const float lap = mul(K.nu, acc);
+    float gr[2];  // Grad(u2, 1.0): row c of the 2x2 matrix
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+      float g = 0.0f;
+#pragma unroll
+      for (int t = 0; t < 3; ++t) g = add(g, mul(K.wd[t], nb[a][c][t]));
+      gr[a] = mul(1.0f, g);
+    }
+    const float conv = add(mul(gr[0], uc[0]), mul(gr[1], uc[1]));
+    res[c] = add(uc[c], mul(K.dt, sub(lap, conv)));
+  }
+}
+
 __global__ void __launch_bounds__(256) ldc_predictor_kernel(const float* __restrict__ u, float* __restrict__ us,
                                                              Geo G, const PdeBCRules Ru, LdcConst K) {
-  const int64_t total = G.n[0] * G.n[1];
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (int)G.n[1]) return;
+  const int n1 = (int)G.n[1];
+  const int cell = i * n1 + j;
   GlobalAcc U{u, G.cstride[0], G.cstride[1], 2};
-  for (int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; cell < total;
-       cell += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = cell / G.n[1], j = cell - i * G.n[1];
-    const float a0 = bc_eval2d(G, Ru, U, i, j, 0), a1 = bc_eval2d(G, Ru, U, i, j, 1);
-    const bool st = i >= G.g && i < G.n[0] - G.g && j >= G.g && j < G.n[1] - G.g;
-    if (!st) {
-      us[cell * 2 + 0] = a0;
-      us[cell * 2 + 1] = a1;
-      continue;
-    }
-    float nb[2][2][3];  // [axis][comp][tap]
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      nb[0][c][1] = c == 0 ? a0 : a1;
-      nb[1][c][1] = nb[0][c][1];
-      nb[0][c][0] = bc_eval2d(G, Ru, U, i - 1, j, c);
-      nb[0][c][2] = bc_eval2d(G, Ru, U, i + 1, j, c);
-      nb[1][c][0] = bc_eval2d(G, Ru, U, i, j - 1, c);
-      nb[1][c][2] = bc_eval2d(G, Ru, U, i, j + 1, c);
-    }
-    const float uc[2] = {a0, a1};
-    float res[2];
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      float acc = 0.0f;  // Laplacian, FDM/kernel/laplacian.py:40-46 order
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int t = 0; t < 3; ++t) acc = add(acc, mul(K.wl[t], nb[a][c][t]));
-      const float lap = mul(K.nu, acc);
-      float gr[2];  // Grad(u2, 1.0): row c of the 2x2 matrix
-#pragma unroll
-      for (int a = 0; a < 2; ++a) {
-        float g = 0.0f;
-#pragma unroll
-        for (int t = 0; t < 3; ++t) g = add(g, mul(K.wd[t], nb[a][c][t]));
-        gr[a] = mul(1.0f, g);
-      }
-      const float conv = add(mul(gr[0], uc[0]), mul(gr[1], uc[1]));
-      res[c] = add(uc[c], mul(K.dt, sub(lap, conv)));
-    }
-    us[cell * 2 + 0] = res[0];
-    us[cell * 2 + 1] = res[1];
+  if (!ldc_stencil(G, i, j)) {
+    us[cell * 2 + 0] = bc_eval2d(G, Ru, U, i, j, 0);
+    us[cell * 2 + 1] = bc_eval2d(G, Ru, U, i, j, 1);
+    return;
   }
+  float res[2];
+  if (ldc_deep(G, i, j)) ldc_predict_cell(Raw2<2>{u, n1}, i, j, K, res);
+  else ldc_predict_cell(Bc2{G, Ru, U}, i, j, K, res);
+  us[cell * 2 + 0] = res[0];
+  us[cell * 2 + 1] = res[1];
 }
 
 // rhs = (1/dt) * Div(BC_u(u*)) on stencil cells (ghosts of rhs are never read).
+template <class Get>
+__device__ __forceinline__ float ldc_div_cell(const Get& at, int i, int j, const LdcConst& K) {
+  float acc = 0.0f;  // FDM/kernel/divergence.py:85-106: axis 0 on component 0, axis 1 on component 1
+#pragma unroll
+  for (int t = 0; t < 3; ++t) acc = add(acc, mul(K.wd[t], at(i + t - 1, j, 0)));
+#pragma unroll
+  for (int t = 0; t < 3; ++t) acc = add(acc, mul(K.wd[t], at(i, j + t - 1, 1)));
+  return mul(K.inv_dt, acc);
+}
+
 __global__ void __launch_bounds__(256) ldc_divergence_kernel(const float* __restrict__ us, float* __restrict__ rhs,
                                                               Geo G, const PdeBCRules Ru, LdcConst K) {
-  const int64_t total = G.n[0] * G.n[1];
-  GlobalAcc U{us, G.cstride[0], G.cstride[1], 2};
-  for (int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; cell < total;
-       cell += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = cell / G.n[1], j = cell - i * G.n[1];
-    const bool st = i >= G.g && i < G.n[0] - G.g && j >= G.g && j < G.n[1] - G.g;
-    if (!st) {
-      rhs[cell] = 0.0f;
-      continue;
-    }
-    float acc = 0.0f;  // FDM/kernel/divergence.py:85-106: axis 0 on component 0, axis 1 on component 1
-#pragma unroll
-    for (int t = 0; t < 3; ++t) acc = add(acc, mul(K.wd[t], bc_eval2d(G, Ru, U, i + t - 1, j, 0)));
-#pragma unroll
-    for (int t = 0; t < 3; ++t) acc = add(acc, mul(K.wd[t], bc_eval2d(G, Ru, U, i, j + t - 1, 1)));
-    rhs[cell] = mul(K.inv_dt, acc);
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (int)G.n[1]) return;
+  const int n1 = (int)G.n[1];
+  const int cell = i * n1 + j;
+  if (!ldc_stencil(G, i, j)) {
+    rhs[cell] = 0.0f;
+    return;
   }
+  GlobalAcc U{us, G.cstride[0], G.cstride[1], 2};
+  rhs[cell] = ldc_deep(G, i, j) ? ldc_div_cell(Raw2<2>{us, n1}, i, j, K) : ldc_div_cell(Bc2{G, Ru, U}, i, j, K);
 }
 
 // u = BC_u(u*) + dt * Grad(BC_p(p), -1)
+template <class GetU, class GetP>
+__device__ __forceinline__ void ldc_project_cell(const GetU& au, const GetP& ap, int i, int j, const LdcConst& K,
+                                                 float* res) {
+  const float a0 = au(i, j, 0), a1 = au(i, j, 1);
+  float gx = 0.0f, gy = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 3; ++t) gx = add(gx, mul(K.wd[t], ap(i + t - 1, j, 0)));
+#pragma unroll
+  for (int t = 0; t < 3; ++t) gy = add(gy, mul(K.wd[t], ap(i, j + t - 1, 0)));
+  res[0] = add(a0, mul(K.dt, mul(-1.0f, gx)));
+  res[1] = add(a1, mul(K.dt, mul(-1.0f, gy)));
+}
+
 __global__ void __launch_bounds__(256) ldc_project_kernel(const float* __restrict__ us, const float* __restrict__ p,
                                                            float* __restrict__ u, Geo G, const PdeBCRules Ru,
                                                            const PdeBCRules Rp, LdcConst K) {
-  const int64_t total = G.n[0] * G.n[1];
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (int)G.n[1]) return;
+  const int n1 = (int)G.n[1];
+  const int cell = i * n1 + j;
   GlobalAcc U{us, G.cstride[0], G.cstride[1], 2};
   GlobalAcc Pa{p, G.cstride[0], G.cstride[1], 1};
-  for (int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; cell < total;
-       cell += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = cell / G.n[1], j = cell - i * G.n[1];
-    const float a0 = bc_eval2d(G, Ru, U, i, j, 0), a1 = bc_eval2d(G, Ru, U, i, j, 1);
-    const bool st = i >= G.g && i < G.n[0] - G.g && j >= G.g && j < G.n[1] - G.g;
-    if (!st) {
-      u[cell * 2 + 0] = a0;
-      u[cell * 2 + 1] = a1;
-      continue;
-    }
-    float gx = 0.0f, gy = 0.0f;
-#pragma unroll
-    for (int t = 0; t < 3; ++t) gx = add(gx, mul(K.wd[t], bc_eval2d(G, Rp, Pa, i + t - 1, j, 0)));
-#pragma unroll
-    for (int t = 0; t < 3; ++t) gy = add(gy, mul(K.wd[t], bc_eval2d(G, Rp, Pa, i, j + t - 1, 0)));
-    u[cell * 2 + 0] = add(a0, mul(K.dt, mul(-1.0f, gx)));
-    u[cell * 2 + 1] = add(a1, mul(K.dt, mul(-1.0f, gy)));
+  if (!ldc_stencil(G, i, j)) {
+    u[cell * 2 + 0] = bc_eval2d(G, Ru, U, i, j, 0);
+    u[cell * 2 + 1] = bc_eval2d(G, Ru, U, i, j, 1);
+    return;
   }
+  float res[2];
+  if (ldc_deep(G, i, j)) ldc_project_cell(Raw2<2>{us, n1}, Raw2<1>{p, n1}, i, j, K, res);
+  else ldc_project_cell(Bc2{G, Ru, U}, Bc2{G, Rp, Pa}, i, j, K, res);
+  u[cell * 2 + 0] = res[0];
+  u[cell * 2 + 1] = res[1];
 }
 
 // k Jacobi sweeps per pass on shared-memory tiles (halo k + 1, as in
@@ -144,58 +184,74 @@ __global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restric
   const int H = P.k + 1;
   const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, P.X);
   const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
-  const int RX = rx1 - rx0, RY = ry1 - ry0;
+  const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
+  const int cap = P.RXM * P.RYM;
   float* A = sm;
-  float* B = sm + P.RXM * P.RYM;
-  float* Rh = sm + 2 * P.RXM * P.RYM;
-  // 2D thread layout: 32 lanes along y (contiguous), blockDim.x / 32 rows along x
-  const int ly0 = threadIdx.x & 31, lx0 = threadIdx.x >> 5, nrows = blockDim.x >> 5;
-  for (int lx = lx0; lx < RX; lx += nrows)
-    for (int ly = ly0; ly < RY; ly += 32) {
-      const size_t gi = (size_t)(rx0 + lx) * P.Y + ry0 + ly;
-      A[lx * RY + ly] = __ldg(pin + gi);
-      Rh[lx * RY + ly] = __ldg(rhs + gi);
-    }
+  float* B = sm + cap;
+  float* Rh = sm + 2 * cap;
+  const int nt = (int)blockDim.x;
+  // Both level buffers start with the region (cp.async, every copy of a thread
+  // in flight at once); a sweep writes only its stencil rectangle, so the other
+  // cells keep their loaded or last boundary-filled value.
+  for (int i = threadIdx.x; i < RC; i += nt) {
+    const int lx = i / RY, ly = i - lx * RY;
+    const size_t gi = (size_t)(rx0 + lx) * P.Y + ry0 + ly;
+    cp_async4(A + i, pin + gi, true);
+    cp_async4(B + i, pin + gi, true);
+    cp_async4(Rh + i, rhs + gi, true);
+  }
+  cp_async_wait_all();
   __syncthreads();
   H2Params HP;
   HP.X = P.X; HP.Y = P.Y; HP.g = P.g; HP.N = 1;
   const int g = P.g;
-  // stencil cells of the region whose four neighbours are inside it
+  // stencil rectangle: cells of [g, n-g) whose four neighbours are inside the region
   const int sx0 = max(g, rx0 + 1) - rx0, sx1 = min(P.X - g, rx0 + RX - 1) - rx0;
   const int sy0 = max(g, ry0 + 1) - ry0, sy1 = min(P.Y - g, ry0 + RY - 1) - ry0;
+  const int SW = max(sy1 - sy0, 1), SC = max(sx1 - sx0, 0) * max(sy1 - sy0, 0);
+  const int dq = nt / SW, dr = nt - dq * SW;
+  // the tile in rectangle coordinates (residual cells)
+  const int tx0 = bx0 - rx0 - sx0, ty0 = by0 - ry0 - sy0;
+  const int tw = min(bx0 + P.TBX, P.X) - bx0, th = min(by0 + P.TBY, P.Y) - by0;
   float sq = 0.0f;
   for (int s = 0; s < P.k; ++s) {
     bc_fill_region<1>(A, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);
     const bool acc_res = P.last && s == P.k - 1;
-    for (int lx = lx0; lx < RX; lx += nrows)
-      for (int ly = ly0; ly < RY; ly += 32) {
-        const int idx = lx * RY + ly;
-        const float c = A[idx];
-        float res = c;
-        if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
-          const float sum = add(add(add(A[idx - RY], A[idx + RY]), A[idx - 1]), A[idx + 1]);
-          res = mul(0.25f, sub(sum, mul(P.h2, Rh[idx])));
-          const int x = rx0 + lx, y = ry0 + ly;
-          if (acc_res && x >= bx0 && x < bx0 + P.TBX && y >= by0 && y < by0 + P.TBY) {
-            const float d = res - c;
-            sq = fmaf(d, d, sq);
-          }
+    int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
+    for (int c = threadIdx.x; c < SC; c += nt) {
+      const int i = (sx0 + lx) * RY + sy0 + ly;
+      const float old = A[i];
+      const float sum = add(add(add(A[i - RY], A[i + RY]), A[i - 1]), A[i + 1]);
+      const float res = mul(0.25f, sub(sum, mul(P.h2, Rh[i])));
+      B[i] = res;
+      if (acc_res) {
+        const int ox = lx - tx0, oy = ly - ty0;
+        if (ox >= 0 && ox < tw && oy >= 0 && oy < th) {
+          const float d = res - old;
+          sq = fmaf(d, d, sq);
         }
-        B[idx] = res;
       }
+      lx += dq;
+      ly += dr;
+      if (ly >= SW) { ly -= SW; ++lx; }
+    }
     __syncthreads();
     float* t = A;
     A = B;
     B = t;
   }
-  const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
-  for (int lx = lx0; lx < ox1 - bx0; lx += nrows)
-    for (int ly = ly0; ly < oy1 - by0; ly += 32)
-      pout[(size_t)(bx0 + lx) * P.Y + by0 + ly] = A[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+  // output: stencil cells from the newest level, the others as last filled (B)
+  for (int i = threadIdx.x; i < tw * th; i += nt) {
+    const int lx = i / th, ly = i - lx * th;
+    const int x = bx0 + lx, y = by0 + ly;
+    const int ri = (x - rx0) * RY + (y - ry0);
+    const bool st = x >= g && x < P.X - g && y >= g && y < P.Y - g;
+    pout[(size_t)x * P.Y + y] = st ? A[ri] : B[ri];  // (equal when k = 0: both hold the loaded values)
+  }
   if (P.last && resid) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-    __shared__ float wsum[8];
+    __shared__ float wsum[32];
     if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = sq;
     __syncthreads();
     if (threadIdx.x == 0) {

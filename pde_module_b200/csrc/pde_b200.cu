@@ -153,7 +153,7 @@ int launch_candidate(int cand, const float* in, float* out, const Geo& G, const 
     switch (cand) {
       case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
-      default: return launch_stream3d_k<R, OP, 1, 64, 32, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 5, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
     }
   } else if constexpr (OP == OP_LAP) {
     switch (cand) {
@@ -165,7 +165,7 @@ int launch_candidate(int cand, const float* in, float* out, const Geo& G, const 
     switch (cand) {
       case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
-      default: return launch_stream3d_k<R, OP, 1, 64, 32, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 6, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
     }
   } else {
     switch (cand) {
@@ -854,14 +854,15 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
   K.inv_dt = (float)(1.0 / (double)prm->dt);
   K.h2 = (float)(grid->dx * grid->dx);
   const int64_t cells = G.n[0] * G.n[1];
-  const int blocks = grid_blocks(cells, 256);
+  if (cells >= (1LL << 30) || G.n[0] > 65535) return PDE_ERR_TOO_LARGE;  // 32-bit cell indices, grid rows
+  const dim3 grid2((unsigned)((G.n[1] + 255) / 256), (unsigned)G.n[0]);
   if (resid && nsteps > 0) PDE_CUDA_CHECK(cudaMemsetAsync(resid, 0, sizeof(float) * nsteps, st));
   const int iters = prm->jacobi_iters;
   int k = prm->jacobi_per_pass > 0 ? prm->jacobi_per_pass : 10;
   if (k > iters && iters > 0) k = iters;
   J2Params JP;
   JP.X = (int)G.n[0]; JP.Y = (int)G.n[1]; JP.g = G.g;
-  JP.TBX = 32; JP.TBY = 64;
+  pick_tile_2d(JP.X, JP.Y, &JP.TBX, &JP.TBY);
   JP.tiles_y = (JP.Y + JP.TBY - 1) / JP.TBY;
   JP.RXM = JP.TBX + 2 * (k + 1);
   JP.RYM = JP.TBY + 2 * (k + 1);
@@ -871,8 +872,8 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
   if (jsmem > 227 * 1024) return PDE_ERR_TOO_LARGE;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(jacobi2d_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem));
   for (int step = 0; step < nsteps; ++step) {
-    ldc_predictor_kernel<<<blocks, 256, 0, st>>>(u, u_star, G, *u_rules, K);
-    ldc_divergence_kernel<<<blocks, 256, 0, st>>>(u_star, rhs, G, *u_rules, K);
+    ldc_predictor_kernel<<<grid2, 256, 0, st>>>(u, u_star, G, *u_rules, K);
+    ldc_divergence_kernel<<<grid2, 256, 0, st>>>(u_star, rhs, G, *u_rules, K);
     float* src = p;
     float* dst = p_tmp;
     for (int done = 0; done < iters;) {
@@ -885,7 +886,7 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
       dst = t;
     }
     if (src != p) PDE_CUDA_CHECK(cudaMemcpyAsync(p, src, sizeof(float) * cells, cudaMemcpyDeviceToDevice, st));
-    ldc_project_kernel<<<blocks, 256, 0, st>>>(u_star, p, u, G, *u_rules, *p_rules, K);
+    ldc_project_kernel<<<grid2, 256, 0, st>>>(u_star, p, u, G, *u_rules, *p_rules, K);
     const int rc = launch_status();
     if (rc) return rc;
   }
