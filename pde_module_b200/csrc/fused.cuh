@@ -147,6 +147,10 @@ template <int N>
 __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, const PdeBCRules& Rl, int rx0, int RX,
                                                int ry0, int RY, float dx32) {
   const int g = P.g, X = P.X, Y = P.Y;
+  // A region without ghost or node cells (x, y in [g+1, n-g-2] throughout) has
+  // nothing to fill; the test is the same for every thread of the block, so
+  // the barriers below are skipped by all or by none.
+  if (rx0 > g && rx0 + RX < X - g && ry0 > g && ry0 + RY < Y - g) return;
   const int nthr = blockDim.x, tid = threadIdx.x;
   // ghost strips: x = g-1 (low), x = X-g (high), partner rows y in [g, Y-g)
   const int ylo = max(g, ry0), yhi = min(Y - g, ry0 + RY);
