@@ -138,11 +138,13 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
       // rectangle, so cells outside it keep their loaded or last filled value.
       float* A = sm;  // newest level
       float* B = sm + P.RC;
-      for (int i = threadIdx.x; i < RC; i += nt) {
-        const int lx = i / RY, ly = i - lx * RY;
-        const float* src = in0 + (size_t)(rx0 + lx) * Y + ry0 + ly;
-        cp_async4(A + i, src, true);
-        cp_async4(B + i, src, true);
+      {
+        RectWalk wk(RY, nt);
+        for (int i = threadIdx.x; i < RC; i += nt, wk.next()) {
+          const float* src = in0 + (size_t)(rx0 + wk.row) * Y + ry0 + wk.col;
+          cp_async4(A + i, src, true);
+          cp_async4(B + i, src, true);
+        }
       }
       cp_async_wait_all();
       __syncthreads();
@@ -174,21 +176,23 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
         B = t;
       }
       // output: stencil cells from the newest level, the others as last filled (B)
-      for (int i = threadIdx.x; i < OX * OY; i += nt) {
-        const int lx = i / OY, ly = i - lx * OY;
-        const int x = bx0 + lx, y = by0 + ly;
-        const int ri = (x - rx0) * RY + (y - ry0);
-        const bool st = x >= g && x < X - g && y >= g && y < Y - g;
-        out0[(size_t)x * Y + y] = st ? A[ri] : B[ri];
+      {
+        RectWalk wk(OY, nt);
+        for (int i = threadIdx.x; i < OX * OY; i += nt, wk.next()) {
+          const int x = bx0 + wk.row, y = by0 + wk.col;
+          const int ri = (x - rx0) * RY + (y - ry0);
+          const bool st = x >= g && x < X - g && y >= g && y < Y - g;
+          out0[(size_t)x * Y + y] = st ? A[ri] : B[ri];
+        }
       }
     } else {
       float* Bm = sm;
       float* B0 = sm + P.RC;
       float* Bp = sm + 2 * P.RC;
       // the state is zero outside the node ring (x, y in [g+1, n-g-2]) in every buffer
-      for (int i = threadIdx.x; i < RC; i += nt) {
-        const int lx = i / RY, ly = i - lx * RY;
-        const int x = rx0 + lx, y = ry0 + ly;
+      RectWalk wl(RY, nt);
+      for (int i = threadIdx.x; i < RC; i += nt, wl.next()) {
+        const int x = rx0 + wl.row, y = ry0 + wl.col;
         const bool inside = x > g && x < X - 1 - g && y > g && y < Y - 1 - g;
         const size_t gi = (size_t)x * Y + y;
         cp_async4(Bm + i, in1 + gi, inside);
@@ -224,11 +228,12 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
         B0 = Bp;
         Bp = t;
       }
-      for (int i = threadIdx.x; i < OX * OY; i += nt) {
-        const int lx = i / OY, ly = i - lx * OY;
-        const int ri = (bx0 + lx - rx0) * RY + (by0 + ly - ry0);
-        out1[(size_t)(bx0 + lx) * Y + by0 + ly] = Bm[ri];
-        out0[(size_t)(bx0 + lx) * Y + by0 + ly] = B0[ri];
+      RectWalk wo(OY, nt);
+      for (int i = threadIdx.x; i < OX * OY; i += nt, wo.next()) {
+        const int ri = (bx0 + wo.row - rx0) * RY + (by0 + wo.col - ry0);
+        const size_t gi = (size_t)(bx0 + wo.row) * Y + by0 + wo.col;
+        out1[gi] = Bm[ri];
+        out0[gi] = B0[ri];
       }
     }
     __threadfence();

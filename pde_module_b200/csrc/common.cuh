@@ -16,6 +16,24 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
 // Wait for this thread's cp.async copies (the block still needs a barrier before others read them).
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Walk of a row-major (rows x W) rectangle by a block: cell c = tid, tid + nt, ...
+// as (row, col), advanced without division.
+struct RectWalk {
+  int row, col, dq, dr, W;
+  __device__ RectWalk(int W_, int nt) : W(max(W_, 1)) {
+    dq = nt / W;
+    dr = nt - dq * W;
+    row = (int)threadIdx.x / W;
+    col = (int)threadIdx.x - row * W;
+  }
+  __device__ void next() {
+    row += dq;
+    col += dr;
+    if (col >= W) { col -= W; ++row; }
+  }
+};
+
+
 
 // Geometry of one (X, Y, Z, N...) array, derived from PdeGrid.
 struct Geo {

@@ -50,6 +50,49 @@ __device__ __forceinline__ bool heat_stencil_cell(int x, int y, int X, int Y, in
   return x >= g && x < X - g && y >= g && y < Y - g;
 }
 
+// k forward steps on the stencil rectangle; STORE: S^{n0+s} of the tile's cells.
+template <int R, bool STORE>
+__device__ __forceinline__ float* heat_field_steps(const HAParams& P, const PdeBCRules& Rl, float* A, float* B,
+                                                   const float* AL, int rx0, int RX, int ry0, int RY, int bx0,
+                                                   int by0, int OX, int OY) {
+  H2Params HP;
+  HP.X = P.X; HP.Y = P.Y; HP.g = P.g; HP.N = 1;
+  const int g = P.g, X = P.X, Y = P.Y;
+  const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
+  const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
+  const int SW = max(sy1 - sy0, 1), SC = max(sx1 - sx0, 0) * max(sy1 - sy0, 0);
+  const int nt = (int)blockDim.x;
+  const int dq = nt / SW, dr = nt - dq * SW;
+  const int tx0 = bx0 - rx0 - sx0, ty0 = by0 - ry0 - sy0;  // the tile in rectangle coordinates
+  for (int s = 0; s < P.k; ++s) {
+    bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
+    int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
+    for (int c = threadIdx.x; c < SC; c += nt) {
+      const int i = (sx0 + lx) * RY + sy0 + ly;
+      const float u2 = A[i];
+      float acc = 0.0f;
+#pragma unroll
+      for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[i + (t - R) * RY]));
+#pragma unroll
+      for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[i + (t - R)]));
+      B[i] = add(u2, mul(P.dt, mul(AL[i], acc)));
+      if (STORE) {
+        const int ox = lx - tx0, oy = ly - ty0;
+        if (ox >= 0 && ox < OX && oy >= 0 && oy < OY) Ls[(size_t)(bx0 + ox) * Y + by0 + oy] = acc;
+      }
+      lx += dq;
+      ly += dr;
+      if (ly >= SW) { ly -= SW; ++lx; }
+    }
+    __syncthreads();
+    float* t = A;
+    A = B;
+    B = t;
+  }
+  return A;
+}
+
 template <int R>
 __global__ void __launch_bounds__(256) heat2d_field_fwd_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                                 const HAParams P, const PdeBCRules Rl) {
@@ -61,53 +104,32 @@ __global__ void __launch_bounds__(256) heat2d_field_fwd_kernel(const float* __re
   const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, X);
   const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, Y);
   const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
-  float* A = sm;
-  float* B = sm + P.RC;
+  const int OX = min(bx0 + P.TBX, X) - bx0, OY = min(by0 + P.TBY, Y) - by0;
+  // Both level buffers start with the region; a step writes only its stencil
+  // rectangle, so the other cells keep their loaded or last filled value.
+  float* A0 = sm;
+  float* B0 = sm + P.RC;
   float* AL = sm + 2 * P.RC;
-  for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-    const int lx = i / RY, ly = i - lx * RY;
-    const size_t gi = (size_t)(rx0 + lx) * Y + ry0 + ly;
-    cp_async4(A + i, in + gi, true);
-    cp_async4(AL + i, P.alpha + gi, true);
+  {
+    RectWalk wk(RY, (int)blockDim.x);
+    for (int i = threadIdx.x; i < RC; i += blockDim.x, wk.next()) {
+      const size_t gi = (size_t)(rx0 + wk.row) * Y + ry0 + wk.col;
+      cp_async4(A0 + i, in + gi, true);
+      cp_async4(B0 + i, in + gi, true);
+      cp_async4(AL + i, P.alpha + gi, true);
+    }
   }
   cp_async_wait_all();
   __syncthreads();
-  H2Params HP;
-  HP.X = X; HP.Y = Y; HP.g = g; HP.N = 1;
-  const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
-  const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
-  const int ox1 = min(bx0 + P.TBX, X), oy1 = min(by0 + P.TBY, Y);
-  const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
-  for (int s = 0; s < P.k; ++s) {
-    bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, Rl.dx32);
-    float* Ls = P.lst ? P.lst + (size_t)s * P.cells : nullptr;
-    int lx = (int)threadIdx.x / RY, ly = (int)threadIdx.x - lx * RY;
-    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-      const float u2 = A[i];
-      float res = u2, acc = 0.0f;
-      if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
-#pragma unroll
-        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[i + (t - R) * RY]));
-#pragma unroll
-        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[i + (t - R)]));
-        res = add(u2, mul(P.dt, mul(AL[i], acc)));
-      }
-      B[i] = res;
-      const int x = rx0 + lx, y = ry0 + ly;
-      if (Ls && x >= bx0 && x < ox1 && y >= by0 && y < oy1) Ls[(size_t)x * Y + y] = acc;
-      lx += dq;
-      ly += dr;
-      if (ly >= RY) { ly -= RY; ++lx; }
-    }
-    __syncthreads();
-    float* t = A;
-    A = B;
-    B = t;
-  }
-  const int OX = ox1 - bx0, OY = oy1 - by0;
-  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
-    const int lx = i / OY, ly = i - lx * OY;
-    out[(size_t)(bx0 + lx) * Y + by0 + ly] = A[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+  float* A = P.lst ? heat_field_steps<R, true>(P, Rl, A0, B0, AL, rx0, RX, ry0, RY, bx0, by0, OX, OY)
+                   : heat_field_steps<R, false>(P, Rl, A0, B0, AL, rx0, RX, ry0, RY, bx0, by0, OX, OY);
+  const float* Bf = (A == A0) ? B0 : A0;  // the last boundary-filled level
+  // output: stencil cells from the newest level, the others as last filled
+  RectWalk wo(OY, (int)blockDim.x);
+  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x, wo.next()) {
+    const int x = bx0 + wo.row, y = by0 + wo.col;
+    const int ri = (x - rx0) * RY + (y - ry0);
+    out[(size_t)x * Y + y] = heat_stencil_cell(x, y, X, Y, g) ? A[ri] : Bf[ri];
   }
 }
 
@@ -171,27 +193,28 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
   const int OT = OX * OY;
   auto fetch_S = [&](int s, int slot) {
     const float* Sn = P.lsts + (size_t)(P.ntop - s) * P.cells;
-    for (int i = threadIdx.x; i < OT; i += blockDim.x) {
-      const int lx = i / OY, ly = i - lx * OY;
-      cp_async4(GL + slot * OT + i, Sn + (size_t)(bx0 + lx) * Y + by0 + ly, true);
-    }
+    RectWalk wk(OY, (int)blockDim.x);
+    for (int i = threadIdx.x; i < OT; i += blockDim.x, wk.next())
+      cp_async4(GL + slot * OT + i, Sn + (size_t)(bx0 + wk.row) * Y + by0 + wk.col, true);
   };
   const float dt = P.dt;
-  for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-    const int lx = i / RY, ly = i - lx * RY;
-    const size_t gi = (size_t)(rx0 + lx) * Y + ry0 + ly;
-    cp_async4(Lm + i, lam_in + gi, true);
-    cp_async4(AL + i, P.alpha + gi, true);
-  }
-  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
-    const int lx = i / OY, ly = i - lx * OY;
-    cp_async4(GA + i, P.galpha + (size_t)(bx0 + lx) * Y + by0 + ly, true);
+  {
+    RectWalk wk(RY, (int)blockDim.x);
+    for (int i = threadIdx.x; i < RC; i += blockDim.x, wk.next()) {
+      const size_t gi = (size_t)(rx0 + wk.row) * Y + ry0 + wk.col;
+      cp_async4(Lm + i, lam_in + gi, true);
+      cp_async4(AL + i, P.alpha + gi, true);
+    }
+    RectWalk wt(OY, (int)blockDim.x);
+    for (int i = threadIdx.x; i < OX * OY; i += blockDim.x, wt.next())
+      cp_async4(GA + i, P.galpha + (size_t)(bx0 + wt.row) * Y + by0 + wt.col, true);
   }
   fetch_S(0, 0);
   cp_async_wait_all();
-  for (int i = threadIdx.x; i < RC; i += blockDim.x) {  // the cells this thread copied
-    const int lx = i / RY, ly = i - lx * RY;
-    Z[i] = heat_stencil_cell(rx0 + lx, ry0 + ly, X, Y, g) ? mul(dt, mul(AL[i], Lm[i])) : 0.0f;
+  {
+    RectWalk wk(RY, (int)blockDim.x);  // the cells this thread copied
+    for (int i = threadIdx.x; i < RC; i += blockDim.x, wk.next())
+      Z[i] = heat_stencil_cell(rx0 + wk.row, ry0 + wk.col, X, Y, g) ? mul(dt, mul(AL[i], Lm[i])) : 0.0f;
   }
   __syncthreads();
   const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
@@ -248,10 +271,10 @@ __global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict
     cp_async_wait_all();  // this thread's copies of the next step's S; the barrier publishes them
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x) {
-    const int lx = i / OY, ly = i - lx * OY;
-    const size_t gi = (size_t)(bx0 + lx) * Y + by0 + ly;
-    lam_out[gi] = Lm[(bx0 + lx - rx0) * RY + (by0 + ly - ry0)];
+  RectWalk wo(OY, (int)blockDim.x);
+  for (int i = threadIdx.x; i < OX * OY; i += blockDim.x, wo.next()) {
+    const size_t gi = (size_t)(bx0 + wo.row) * Y + by0 + wo.col;
+    lam_out[gi] = Lm[(bx0 + wo.row - rx0) * RY + (by0 + wo.col - ry0)];
     P.galpha[gi] = GA[i];
   }
 }

@@ -193,12 +193,14 @@ __global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restric
   // Both level buffers start with the region (cp.async, every copy of a thread
   // in flight at once); a sweep writes only its stencil rectangle, so the other
   // cells keep their loaded or last boundary-filled value.
-  for (int i = threadIdx.x; i < RC; i += nt) {
-    const int lx = i / RY, ly = i - lx * RY;
-    const size_t gi = (size_t)(rx0 + lx) * P.Y + ry0 + ly;
-    cp_async4(A + i, pin + gi, true);
-    cp_async4(B + i, pin + gi, true);
-    cp_async4(Rh + i, rhs + gi, true);
+  {
+    RectWalk wk(RY, nt);
+    for (int i = threadIdx.x; i < RC; i += nt, wk.next()) {
+      const size_t gi = (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col;
+      cp_async4(A + i, pin + gi, true);
+      cp_async4(B + i, pin + gi, true);
+      cp_async4(Rh + i, rhs + gi, true);
+    }
   }
   cp_async_wait_all();
   __syncthreads();
@@ -241,9 +243,9 @@ __global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restric
     B = t;
   }
   // output: stencil cells from the newest level, the others as last filled (B)
-  for (int i = threadIdx.x; i < tw * th; i += nt) {
-    const int lx = i / th, ly = i - lx * th;
-    const int x = bx0 + lx, y = by0 + ly;
+  RectWalk wo(th, nt);
+  for (int i = threadIdx.x; i < tw * th; i += nt, wo.next()) {
+    const int x = bx0 + wo.row, y = by0 + wo.col;
     const int ri = (x - rx0) * RY + (y - ry0);
     const bool st = x >= g && x < P.X - g && y >= g && y < P.Y - g;
     pout[(size_t)x * P.Y + y] = st ? A[ri] : B[ri];  // (equal when k = 0: both hold the loaded values)

@@ -79,23 +79,6 @@ struct WaveRect {
   }
 };
 
-// Walk of a row-major (rows x W) rectangle by a block: cell c = tid, tid + nt, ...
-// as (row, col), advanced without division.
-struct RectWalk {
-  int row, col, dq, dr, W;
-  __device__ RectWalk(int W_, int nt) : W(max(W_, 1)) {
-    dq = nt / W;
-    dr = nt - dq * W;
-    row = (int)threadIdx.x / W;
-    col = (int)threadIdx.x - row * W;
-  }
-  __device__ void next() {
-    row += dq;
-    col += dr;
-    if (col >= W) { col -= W; ++row; }
-  }
-};
-
 // Load a region row-major (RX x RY) with fn(region index, array x, array y).
 template <class F>
 __device__ __forceinline__ void for_region(const WaveRegion& Rg, F fn) {
