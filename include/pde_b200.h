@@ -229,8 +229,8 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
  * Forward step with a per-cell diffusivity field alpha (X, Y):
  *   v = BC(u);  S = Lap(v) (alpha 1);  u' = v + dt*(alpha o S) on stencil cells, v elsewhere
  * (bit-identical to pde_heat_rollout when alpha is constant).  `lstates`, if
- * not NULL, receives S of step n at lstates + n*X*Y for n = 0..nsteps-1 (0
- * off the stencil cells).  `work`: one field of scratch. */
+ * not NULL, receives S of step n at lstates + n*X*Y for n = 0..nsteps-1 on the
+ * stencil cells (other cells unspecified).  `work`: one field of scratch. */
 int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
                      const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
                      void* stream);
@@ -286,9 +286,21 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
 int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out,
                      float* mu_out_next, const float* lstates, float* grad_K, int32_t nsteps,
                      int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
+/* pde_wave_forward (nsteps_fwd steps from n0, L(u^n) stored to lstates_fwd; the
+ * final state is not returned) and pde_wave_adjoint (nsteps_adj steps from
+ * lstates_adj, grad_K accumulated) of two different segments in one sequence of
+ * paired launches: each launch advances every tile through up to
+ * steps_per_pass steps of both, so the two interleave on each SM.  Results are
+ * bit-identical to the two calls made separately.  Either step count may be 0
+ * (that part's pointers may then be NULL).  The pass depth is steps_per_pass or
+ * the deepest below it whose shared-memory region fits.  work: 6 fields. */
+int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32_t n0, int32_t nsteps_fwd,
+                  float* lstates_fwd, const float* mu_next, const float* mu_next2, float* mu_out, float* mu_out_next,
+                  const float* lstates_adj, float* grad_K, int32_t nsteps_adj, const float* src, int64_t src_cell,
+                  int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
 /* Launch shape of the temporally blocked 2D kernels of pde_heat_forward,
- * pde_heat_adjoint, pde_wave_forward, pde_wave_adjoint and the Jacobi sweeps of
- * pde_ldc_rollout, process-wide:
+ * pde_heat_adjoint, pde_wave_forward, pde_wave_adjoint, pde_wave_pair and the
+ * Jacobi sweeps of pde_ldc_rollout, process-wide:
  * output tile (sides 8..256; (0, 0) = automatic: the largest of 32x64, 32x32,
  * 16x32 that gives every SM a tile) and threads per block of the wave kernels
  * (256, 512, 1024; 0 = automatic: 1024 with up to 1.1 tiles per SM, 512 up to

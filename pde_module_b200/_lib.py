@@ -127,6 +127,9 @@ _SIGS = {
                                    C.POINTER(PdeGrid), C.c_void_p]),
     "pde_wave_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.POINTER(PdeGrid), C.c_void_p]),
+    "pde_wave_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.POINTER(PdeGrid), C.c_void_p]),
     "pde_set_launch_2d": (C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
     "pde_heat_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid),
                                    C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32, C.c_void_p,

@@ -787,6 +787,84 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
   return PDE_OK;
 }
 
+int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32_t n0, int32_t nsteps_fwd,
+                  float* lstates_fwd, const float* mu_next, const float* mu_next2, float* mu_out, float* mu_out_next,
+                  const float* lstates_adj, float* grad_K, int32_t nsteps_adj, const float* src, int64_t src_cell,
+                  int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream) {
+  if (!K || !work || !grid || nsteps_fwd < 0 || nsteps_adj < 0 || n0 < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
+  if (nsteps_fwd > 0 && (!u_prev || !u_cur || !lstates_fwd)) return PDE_ERR_ARG;
+  if (nsteps_adj > 0 && (!mu_next || !mu_next2 || !mu_out || !mu_out_next || !lstates_adj || !grad_K))
+    return PDE_ERR_ARG;
+  if (src_cell >= 0 && !src) return PDE_ERR_ARG;
+  const int nmax = nsteps_fwd > nsteps_adj ? nsteps_fwd : nsteps_adj;
+  if (nmax == 0) return PDE_OK;
+  Geo G;
+  WaveParams Pa;
+  int k;
+  size_t smem;
+  // results do not depend on the pass depth: take the deepest one (up to the
+  // requested) whose nine region buffers fit in shared memory
+  bool ok = false;
+  for (int kk = steps_per_pass > 0 ? steps_per_pass : 8; kk >= 1 && !ok; --kk)
+    ok = wave_setup(grid, kk, nmax, &G, &Pa, &k, &smem, 9, 1);
+  if (!ok) return PDE_ERR_UNSUPPORTED;
+  if (src_cell >= Pa.cells) return PDE_ERR_ARG;
+  WaveParams Pf = Pa;
+  if (src_cell >= 0) {
+    Pf.srcx = (int)(src_cell / Pf.Y);
+    Pf.srcy = (int)(src_cell % Pf.Y);
+    Pf.src = src;
+  }
+  Pa.lsts = lstates_adj;
+  Pa.gK = grad_K;
+  cudaStream_t st = as_stream(stream);
+  const size_t bytes = sizeof(float) * (size_t)Pa.cells;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_pair_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int tiles = ((Pa.X + Pa.TBX - 1) / Pa.TBX) * Pa.tiles_y;
+  const int threads = pick_threads_2d(tiles);
+  float* w[6];
+  for (int i = 0; i < 6; ++i) w[i] = work + (size_t)i * Pa.cells;
+  // forward part: (u_prev, u_cur) -> (w0, w1) -> (w2, w3) -> (w0, w1) ...; the inputs are never written
+  const float* fa = u_prev;
+  const float* fb = u_cur;
+  int fslot = 0;
+  // adjoint part: alternate (w4, w5) and the outputs so that its last pass writes the outputs
+  const int npa = (nsteps_adj + k - 1) / k;
+  const bool alias = mu_out == mu_next || mu_out_next == mu_next2 || mu_out == mu_next2 || mu_out_next == mu_next;
+  bool to_out = alias ? false : (npa % 2 == 1);
+  const float* ma = mu_next;
+  const float* mb = mu_next2;
+  for (int done = 0; done < nmax; done += k) {
+    Pf.k = nsteps_fwd - done < k ? (nsteps_fwd - done > 0 ? nsteps_fwd - done : 0) : k;
+    Pa.k = nsteps_adj - done < k ? (nsteps_adj - done > 0 ? nsteps_adj - done : 0) : k;
+    Pf.n0 = n0 + done;
+    Pf.lst = Pf.k > 0 ? lstates_fwd + (size_t)done * Pf.cells : nullptr;
+    Pa.ntop = nsteps_adj - 1 - done;
+    float* fo_a = w[2 * fslot];
+    float* fo_b = w[2 * fslot + 1];
+    float* mo_a = to_out ? mu_out : w[4];
+    float* mo_b = to_out ? mu_out_next : w[5];
+    wave_pair_tb_kernel<<<tiles, threads, smem, st>>>(fa, fb, fo_a, fo_b, ma, mb, mo_a, mo_b, K, Pf, Pa);
+    const int rc = launch_status();
+    if (rc) return rc;
+    if (Pf.k > 0) {
+      fa = fo_a;
+      fb = fo_b;
+      fslot ^= 1;
+    }
+    if (Pa.k > 0) {
+      ma = mo_a;
+      mb = mo_b;
+      to_out = !to_out;
+    }
+  }
+  if (nsteps_adj > 0 && ma != mu_out) {
+    PDE_CUDA_CHECK(cudaMemcpyAsync(mu_out, ma, bytes, cudaMemcpyDeviceToDevice, st));
+    PDE_CUDA_CHECK(cudaMemcpyAsync(mu_out_next, mb, bytes, cudaMemcpyDeviceToDevice, st));
+  }
+  return PDE_OK;
+}
+
 int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2, float* mu_out, float* mu_out_next,
                      const float* lstates, float* grad_K, int32_t nsteps, int32_t steps_per_pass, float* work,
                      const PdeGrid* grid, void* stream) {

@@ -232,4 +232,115 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
   });
 }
 
+// ---- paired launch: forward recomputation beside the adjoint --------------
+// One launch advances the same tile through up to k forward steps of one
+// segment (storing L(u^n) of the tile, as wave_fwd_tb_kernel with lst set) and
+// up to k adjoint steps of another segment (as wave_adj_tb_kernel).  The two
+// are independent, so each warp interleaves two dependency chains and a step
+// of both costs one barrier.  Arithmetic and per-cell operation order are
+// those of the two kernels above.  Shared memory (offsets of RC cells): forward
+// levels 0-2, adjoint levels 3-5, K o mu 6-7, K 8, then the gradient tile.
+__global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restrict__ um_in,
+                                                             const float* __restrict__ u0_in,
+                                                             float* __restrict__ um_out, float* __restrict__ u0_out,
+                                                             const float* __restrict__ m1_in,
+                                                             const float* __restrict__ m2_in,
+                                                             float* __restrict__ m1_out, float* __restrict__ m2_out,
+                                                             const float* __restrict__ Kf, const WaveParams Pf,
+                                                             const WaveParams Pa) {
+  extern __shared__ __align__(16) float sm[];
+  const int H = max(Pf.k, Pa.k);
+  const WaveRegion Rg(Pa, H);  // Pf and Pa share the grid, tile and region capacity
+  const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
+  const int RC = Pa.RC;
+  int fm = 0, f0 = RC, fp = 2 * RC;
+  int a2 = 3 * RC, a1 = 4 * RC, a0 = 5 * RC, k1 = 6 * RC, k0 = 7 * RC;
+  const int okk = 8 * RC, oga = 9 * RC;
+  const bool fwd = Pf.k > 0, adj = Pa.k > 0;
+  for_region(Rg, [&](int i, int x, int y) {
+    const size_t gi = (size_t)x * Pa.Y + y;
+    const bool in = wave_inside(Pa, x, y);  // the states are zero outside the node ring
+    cp_async4(sm + okk + i, Kf + gi, true);
+    if (fwd) {
+      cp_async4(sm + fm + i, um_in + gi, in);
+      cp_async4(sm + f0 + i, u0_in + gi, in);
+      sm[fp + i] = 0.0f;
+    }
+    if (adj) {
+      cp_async4(sm + a2 + i, m2_in + gi, in);
+      cp_async4(sm + a1 + i, m1_in + gi, in);
+      sm[a0 + i] = 0.0f;
+      sm[k0 + i] = 0.0f;
+    }
+  });
+  if (adj) for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, Pa.gK + gi, true); });
+  cp_async_wait_all();
+  if (adj) for_region(Rg, [&](int i, int x, int y) { sm[k1 + i] = mul(sm[okk + i], sm[a1 + i]); });
+  __syncthreads();
+  const WaveRect Rt(Pa, Rg);
+  const int nt = (int)blockDim.x;
+  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
+  const int srci = (Pf.srcx >= 0 && Pf.srcx >= rx0 && Pf.srcx < rx0 + Rg.RX && Pf.srcy >= ry0 && Pf.srcy < ry0 + RY)
+                       ? (Pf.srcx - rx0) * RY + (Pf.srcy - ry0) : -1;
+  for (int s = 0; s < H; ++s) {
+    const bool fs = s < Pf.k, as = s < Pa.k;
+    const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
+    float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
+    const float* Ln = as ? Pa.lsts + (size_t)(Pa.ntop - s) * Pa.cells : nullptr;
+    RectWalk wk(Rt.W, nt);
+    for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
+      const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
+      const int ox = wk.row - tx0, oy = wk.col - ty0;
+      const bool tile = ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY;
+      if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+        const float lap = lap5s(sm, f0 + i, RY, Pf.w);
+        float v = sub(mul(2.0f, sm[f0 + i]), sm[fm + i]);
+        v = add(v, mul(sm[okk + i], lap));
+        if (i == srci) v = add(v, sn);
+        sm[fp + i] = v;
+        if (tile) Ls[(size_t)(Rg.bx0 + ox) * Pf.Y + Rg.by0 + oy] = lap;
+      }
+      if (as) {
+        const float m1 = sm[a1 + i];
+        if (tile) {  // dJ/dK += mu^{n+1} o L(u^n)
+          const int t = oga + ox * Rg.OY + oy;
+          sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * Pa.Y + Rg.by0 + oy)));
+        }
+        // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+        const float acc = lap5s(sm, k1 + i, RY, Pa.w);
+        const float v = add(sub(mul(2.0f, m1), sm[a2 + i]), acc);
+        sm[a0 + i] = v;
+        sm[k0 + i] = mul(sm[okk + i], v);
+      }
+    }
+    __syncthreads();
+    if (fs) {
+      const int t = fm;
+      fm = f0;
+      f0 = fp;
+      fp = t;
+    }
+    if (as) {
+      int t = a2;
+      a2 = a1;
+      a1 = a0;
+      a0 = t;
+      t = k1;
+      k1 = k0;
+      k0 = t;
+    }
+  }
+  for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) {
+    if (fwd) {
+      um_out[gi] = sm[fm + ri];
+      u0_out[gi] = sm[f0 + ri];
+    }
+    if (adj) {
+      m1_out[gi] = sm[a1 + ri];
+      m2_out[gi] = sm[a2 + ri];
+      Pa.gK[gi] = sm[oga + t];
+    }
+  });
+}
+
 }  // namespace pde

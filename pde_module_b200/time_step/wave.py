@@ -79,11 +79,11 @@ class WaveSolver:
             return
         dev, f = like.device, self.shape + (1,)
         z = lambda *s: torch.zeros(s, dtype=torch.float32, device=dev)
-        self._work = z(2, self.shape[0] * self.shape[1])
-        self._work_r = z(2, self.shape[0] * self.shape[1])   # the recomputation's own scratch
+        self._work = z(6, self.shape[0] * self.shape[1])
         self._seg = z(max(self.every, 1), self.shape[0] * self.shape[1])
+        # a second buffer of L(u^n): the recomputation of segment j-1 fills it while
+        # the adjoint of segment j reads the first
         self._seg2 = z(max(self.every, 1), self.shape[0] * self.shape[1]) if len(self.segments) > 1 else self._seg
-        self._side = torch.cuda.Stream(device=dev)
         self._K, self._u0, self._g = z(*f), z(*f), z(*f)
         self._ck = z(max(len(self.segments), 1), 2, *f)       # (u^{n0-1}, u^{n0}) per segment
         self._out = z(2, *f)                                   # (u^{N-1}, u^N)
@@ -120,42 +120,30 @@ class WaveSolver:
             self._out[1].copy_(self._u0)
 
     def _run_backward(self) -> None:
-        """Segments from the last to the first.  The adjoint of segment j (this
-        stream) runs while a second stream recomputes L(u^n) of segment j-1 into
-        the other of two buffers; events order each buffer's reuse."""
-        main, side = torch.cuda.current_stream(), self._side
+        """Segments from the last to the first, each one paired launch sequence
+        (pde_wave_pair): the adjoint of segment j beside the recomputation of
+        L(u^n) of segment j-1 into the other of two buffers."""
         J = len(self.segments) - 1
         bufs = (self._seg, self._seg2)  # segment j uses bufs[(J - j) % 2]; the forward filled bufs[0]
         self._gK.zero_()
         a, b = self._mu[0], self._mu[1]
         a[0].copy_(self._g)
         a[1].zero_()
-        side.wait_stream(main)
-        rec_done, adj_done = {}, {}
+        P = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
         for j in range(J, -1, -1):
-            if j >= 1:  # recompute L(u^{n0}) .. L(u^{n0+m-1}) of segment j-1 from its checkpoint
-                n0, m = self.segments[j - 1]
-                with torch.cuda.stream(side):
-                    if j + 1 in adj_done:
-                        side.wait_event(adj_done[j + 1])  # its buffer was segment j+1's
-                    self._fwd(self._K, self._ck[j - 1, 0], self._ck[j - 1, 1], self._tmp[0], self._tmp[1], n0, m,
-                              lstates=bufs[(J - j + 1) % 2][:m], work=self._work_r)
-                    rec_done[j - 1] = torch.cuda.Event()
-                    rec_done[j - 1].record(side)
             n0, m = self.segments[j]
-            if j in rec_done:
-                main.wait_event(rec_done[j])
-            seg = bufs[(J - j) % 2][:m]
-            check(lib().pde_wave_adjoint(C.c_void_p(self._K.data_ptr()), C.c_void_p(a[0].data_ptr()),
-                                         C.c_void_p(a[1].data_ptr()), C.c_void_p(b[0].data_ptr()),
-                                         C.c_void_p(b[1].data_ptr()), C.c_void_p(seg.data_ptr()),
-                                         C.c_void_p(self._gK.data_ptr()), m, self.steps_per_pass,
-                                         C.c_void_p(self._work.data_ptr()), C.byref(self.grid),
-                                         C.c_void_p(main.cuda_stream)), "pde_wave_adjoint")
-            adj_done[j] = torch.cuda.Event()
-            adj_done[j].record(main)
+            if j >= 1:
+                f0, fm = self.segments[j - 1]
+                ck, lf = self._ck[j - 1], bufs[(J - j + 1) % 2][:fm]
+            else:
+                f0, fm, ck, lf = 0, 0, None, None
+            check(lib().pde_wave_pair(P(self._K), P(ck[0]) if ck is not None else None,
+                                      P(ck[1]) if ck is not None else None, f0, fm, P(lf),
+                                      P(a[0]), P(a[1]), P(b[0]), P(b[1]), P(bufs[(J - j) % 2][:m]), P(self._gK), m,
+                                      C.c_void_p(self.src.data_ptr()) if self.src_cell >= 0 else None,
+                                      self.src_cell, self.steps_per_pass, P(self._work), C.byref(self.grid),
+                                      C.c_void_p(stream_ptr(self._K))), "pde_wave_pair")
             a, b = b, a
-        main.wait_stream(side)
         torch.sub(a[0], a[1], out=self._gu)  # dJ/du0 = mu^0 + mu^{-1} = mu^0 - mu^1
 
     # -- public ------------------------------------------------------------------

@@ -195,3 +195,24 @@ def test_batch_plan_validation_needs_no_gpu():
     assert plan_rc(r=ramp) == _lib.PDE_ERR_UNSUPPORTED
     assert L.pde_batch_rollout(None, 5, None) == _lib.PDE_ERR_ARG
     assert L.pde_batch_rollout(C.byref(_lib.PdeBatchPlan()), 5, None) == _lib.PDE_ERR_ARG
+
+
+def test_wave_pair_validation_needs_no_gpu():
+    L = _lib.lib()
+    g = _lib.make_grid((20, 20, 1), 1, 2, 0.1)
+    p = C.c_void_p(1 << 20)
+    args = lambda **kw: dict(dict(K=p, up=p, uc=p, n0=0, nf=3, lf=p, m1=p, m2=p, o1=p, o2=p, la=p, gk=p, na=3,
+                                  src=None, cell=-1, k=2, work=p), **kw)
+
+    def call(**kw):
+        a = args(**kw)
+        return L.pde_wave_pair(a["K"], a["up"], a["uc"], a["n0"], a["nf"], a["lf"], a["m1"], a["m2"], a["o1"],
+                               a["o2"], a["la"], a["gk"], a["na"], a["src"], a["cell"], a["k"], a["work"],
+                               C.byref(g), None)
+    assert call(K=None) == _lib.PDE_ERR_ARG
+    assert call(nf=-1) == _lib.PDE_ERR_ARG
+    assert call(lf=None) == _lib.PDE_ERR_ARG
+    assert call(la=None) == _lib.PDE_ERR_ARG
+    assert call(cell=5) == _lib.PDE_ERR_ARG          # a source cell needs source samples
+    assert call(nf=0, na=0) == _lib.PDE_OK           # nothing to do
+    assert call(nf=0, lf=None, up=None, uc=None, na=0) == _lib.PDE_OK

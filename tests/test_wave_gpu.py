@@ -84,3 +84,51 @@ def test_autograd_speed_gradient_matches_float64():
     gu = u0d.grad.cpu().numpy()[:, :, 0, 0]
     relu = np.linalg.norm(gu - u064.grad.numpy()) / np.linalg.norm(u064.grad.numpy())
     assert relu < 1e-3
+
+
+@pytest.mark.parametrize("nf,na,k", [(7, 5, 3), (9, 9, 4), (0, 6, 4), (5, 0, 2), (12, 3, 16)])
+def test_pair_equals_separate_calls(nf, na, k):
+    """pde_wave_pair (forward recomputation of one segment beside the adjoint of
+    another) is bit-identical to pde_wave_forward + pde_wave_adjoint."""
+    import ctypes as C
+    from pde_module_b200 import _lib
+    K, u0, src, cell, N, dx, _, _ = _setup(X=70, Y=90, N=20)
+    X, Y = K.shape[:2]
+    rng = np.random.default_rng(8)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+    inside = interior_mask((X, Y, 1), 1, "cuda")
+    Kd, srcd = dev(K), dev(src)
+    up, uc = dev(u0) * inside, dev(rng.standard_normal((X, Y, 1, 1)) * 1e-3) * inside
+    m1, m2 = dev(rng.standard_normal((X, Y, 1, 1))) * inside, dev(rng.standard_normal((X, Y, 1, 1))) * inside
+    la = dev(rng.standard_normal((max(na, 1), X, Y)))
+    gK0 = dev(rng.standard_normal((X, Y, 1, 1)))
+    grid = _lib.make_grid((X, Y, 1), 1, 2, dx)
+    L = _lib.lib()
+    P = lambda t: C.c_void_p(t.data_ptr())
+    # separate calls
+    lf_ref = torch.zeros((max(nf, 1), X, Y), device="cuda")
+    work = torch.zeros((6, X * Y), device="cuda")
+    o1, o2 = torch.empty_like(uc), torch.empty_like(uc)
+    if nf:
+        _lib.check(L.pde_wave_forward(P(Kd), P(up), P(uc), P(o1), P(o2), P(srcd), cell, 3, nf, k, P(lf_ref),
+                                      P(work), C.byref(grid), None), "fwd")
+    g_ref = gK0.clone()
+    r1, r2 = m1.clone(), m2.clone()
+    if na:
+        r1, r2 = torch.empty_like(m1), torch.empty_like(m2)
+        _lib.check(L.pde_wave_adjoint(P(Kd), P(m1), P(m2), P(r1), P(r2), P(la), P(g_ref), na, k, P(work),
+                                      C.byref(grid), None), "adj")
+    # paired
+    lf = torch.zeros_like(lf_ref)
+    g = gK0.clone()
+    q1, q2 = m1.clone(), m2.clone()
+    if na:
+        q1, q2 = torch.empty_like(m1), torch.empty_like(m2)
+    _lib.check(L.pde_wave_pair(P(Kd), P(up), P(uc), 3, nf, P(lf), P(m1), P(m2), P(q1), P(q2), P(la), P(g), na,
+                               P(srcd), cell, k, P(work), C.byref(grid), None), "pair")
+    torch.cuda.synchronize()
+    ins = inside[:, :, 0, 0].bool()
+    for s in range(nf):  # stored Laplacians are defined on the cells inside the node ring
+        assert torch.equal(lf[s][ins], lf_ref[s][ins]), s
+    assert torch.equal(g, g_ref)
+    assert torch.equal(q1, r1) and torch.equal(q2, r2)
