@@ -302,9 +302,9 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
  * pde_heat_adjoint, pde_wave_forward, pde_wave_adjoint, pde_wave_pair and the
  * Jacobi sweeps of pde_ldc_rollout, process-wide:
  * output tile (sides 8..256; (0, 0) = automatic: the largest of 32x64, 32x32,
- * 16x32 that gives every SM a tile) and threads per block of the wave kernels
- * (256, 512, 1024; 0 = automatic: 1024 with up to 1.1 tiles per SM, 512 up to
- * 2.2, else 256; the heat kernels use 256). */
+ * 16x32 that gives every SM a tile) and threads per block of the wave and
+ * differentiable-heat kernels (256, 512, 1024; 0 = automatic: 1024 with up to
+ * 1.1 tiles per SM, 512 up to 2.2, else 256; the Jacobi sweeps use 256). */
 int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads);
 
 /* ---- batched rollouts (new: the reference advances every grid with its own

@@ -94,7 +94,7 @@ __device__ __forceinline__ float* heat_field_steps(const HAParams& P, const PdeB
 }
 
 template <int R>
-__global__ void __launch_bounds__(256) heat2d_field_fwd_kernel(const float* __restrict__ in, float* __restrict__ out,
+__global__ void __launch_bounds__(1024) heat2d_field_fwd_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                                 const HAParams P, const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];
   const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
@@ -165,7 +165,7 @@ __device__ __forceinline__ float bt_ghost(const PdeBCRules& Rl, float v, float m
 }
 
 template <int R>
-__global__ void __launch_bounds__(256) heat2d_adj_kernel(const float* __restrict__ lam_in,
+__global__ void __launch_bounds__(1024) heat2d_adj_kernel(const float* __restrict__ lam_in,
                                                           float* __restrict__ lam_out, const HAParams P,
                                                           const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];

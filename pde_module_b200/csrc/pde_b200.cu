@@ -633,6 +633,7 @@ int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float*
   auto kern = R == 1 ? heat2d_field_fwd_kernel<1> : heat2d_field_fwd_kernel<2>;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  const int threads = pick_threads_2d(tiles);
   P.alpha = alpha;
   P.dt = dt;
   const int npasses = (nsteps + k - 1) / k;
@@ -643,7 +644,7 @@ int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float*
   for (int p = 0; p < npasses; ++p) {
     P.k = (nsteps - done < k) ? (nsteps - done) : k;
     P.lst = lstates ? lstates + (size_t)done * P.cells : nullptr;
-    kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);
+    kern<<<tiles, threads, smem, st>>>(src, dst, P, *rules);
     rc = launch_status();
     if (rc) return rc;
     done += P.k;
@@ -680,6 +681,7 @@ int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, co
   auto kern = R == 1 ? heat2d_adj_kernel<1> : heat2d_adj_kernel<2>;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  const int threads = pick_threads_2d(tiles);
   P.alpha = alpha;
   P.dt = dt;
   P.lsts = lstates;
@@ -692,7 +694,7 @@ int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, co
   for (int p = 0; p < npasses; ++p) {
     P.k = (nsteps - done < k) ? (nsteps - done) : k;
     P.ntop = nsteps - 1 - done;
-    kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);
+    kern<<<tiles, threads, smem, st>>>(src, dst, P, *rules);
     rc = launch_status();
     if (rc) return rc;
     done += P.k;
