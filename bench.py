@@ -154,6 +154,64 @@ def cpu_sweep_sample(n: int, threads: int, reps: int = 1, min_seconds: float = 0
     return 6 * n ** 3 * done / dt, dt
 
 
+def _timed_cpu(fn, min_seconds: float):
+    t0 = time.perf_counter()
+    n = 0
+    while n == 0 or time.perf_counter() - t0 < min_seconds:
+        fn()
+        n += 1
+    return n, time.perf_counter() - t0
+
+
+def cpu_heat_sample(steps: int = 20, min_seconds: float = 2.0) -> dict:
+    """The 256^2 heat loop on the host (NumPy float32 restatement, one core), per cell-update."""
+    from oracle import fdm
+    n, g = 256, 1
+    dx = 1.0 / n
+    u0 = np.random.default_rng(0).random((n + 2, n + 2, 1, 1)).astype(np.float32)
+    groups = fdm.standard_groups(u0.shape[:3], g, [("ALL", 1, 0.0, (0,))])
+    reps, dt = _timed_cpu(lambda: fdm.heat_rollout(u0, groups, dx, g, 1.0, 0.2 * dx * dx, steps), min_seconds)
+    return {"value": n * n * steps * reps / dt, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{steps} steps of the 256^2 loop x {reps}, NumPy float32 restatement (oracle/fdm.py)"}
+
+
+def cpu_ldc_sample(n: int = 256, min_seconds: float = 2.0) -> dict:
+    """One fractional step (50 Jacobi sweeps) on the host (NumPy float32 composition), per cell-update."""
+    from oracle import fdm
+    g = 1
+    shape = (n + 2 * g, n + 2 * g, 1)
+    dx = 1.0 / (n - 1)
+    u = np.zeros(shape + (2,), dtype=np.float32)
+    p = np.zeros(shape + (1,), dtype=np.float32)
+    ug = fdm.standard_groups(shape, g, [("ALL", 1, 0.0, (0, 1)), ("+Y", 1, 1.0, (0,))])
+    pg = fdm.standard_groups(shape, g, [("ALL", 2, 0.0, (0,))])
+    nu = 0.01
+    dt = 0.2 * min(dx, dx * dx / (4 * nu))
+    reps, t = _timed_cpu(lambda: fdm.ldc_step(u, p, ug, pg, dx, g, nu, dt, 50), min_seconds)
+    return {"value": n * n * reps / t, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"{reps} fractional steps (50 Jacobi sweeps each) on a {n}^2 grid, NumPy float32 "
+                      "composition of the operators (oracle/fdm.py ldc_step); per cell and step"}
+
+
+def cpu_batched_sample(steps: int = 10, min_seconds: float = 2.0) -> dict:
+    """The batched heat workload's first 4 grids on the host, one after the other (NumPy float32)."""
+    from oracle import fdm
+    sides, alpha, u0, dx, dt = batched_problem()
+    grids = range(4)
+    cells = sum(int(sides[i][0]) * int(sides[i][1]) for i in grids)
+
+    def run():
+        for i in grids:
+            u = u0[i][:, :, None, None]
+            groups = fdm.standard_groups(u.shape[:3], 1, [("ALL", 1, 0.0, (0,))])
+            fdm.heat_rollout(u, groups, dx[i], 1, alpha[i], dt[i], steps)
+
+    reps, t = _timed_cpu(run, min_seconds)
+    return {"value": cells * steps * reps / t, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"grids 0-3 of the batch (per-grid loops), {steps} steps x {reps}, NumPy float32 "
+                      "restatement (oracle/fdm.py); per cell-update"}
+
+
 def sweep_config(world: int) -> dict:
     return {"workload": "3D operator sweep 512^3 (Laplacian, Grad, Divergence; order 2 and 4; periodic ghosts)",
             "interior": [N_INT, N_INT, N_INT], "ops_per_step": 6,
@@ -336,15 +394,21 @@ def run_ours(args):
     heat = None
     if rank == 0 and not args.no_heat:
         heat = run_heat()
+        if not args.no_cpu:
+            heat["cpu_baseline"] = cpu_heat_sample()
     ldc = None
     if rank == 0 and not args.no_ldc:
         ldc = run_ldc()
+        if not args.no_cpu:
+            ldc["cpu_baseline"] = cpu_ldc_sample()
     wave = None
     if rank == 0 and not args.no_wave:
         wave = run_wave()
     batched = None
     if rank == 0 and not args.no_batched:
         batched = run_batched(tune=not args.no_tune)
+        if not args.no_cpu:
+            batched["cpu_baseline"] = cpu_batched_sample()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
