@@ -365,6 +365,20 @@ def run_ours(args):
     cells = N_INT ** 3
     ms_step = ms / K
     value = world * cells * len(ops) / (ms_step / 1000.0)
+    # each operator alone: R back-to-back launches between two events (inputs larger than L2)
+    iso = {}
+    R_ISO = 5
+    for name, fn, b in ops:
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(R_ISO):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_iso = e0.elapsed_time(e1) / R_ISO
+        gbs = cells * b / (t_iso / 1000.0) / 1e9
+        iso[name] = {"ms": round(t_iso, 4), "achieved_gbs": round(gbs, 1)}
 
     peak, peak_kind = peaks()
     traffic = traffic_table()
@@ -392,20 +406,20 @@ def run_ours(args):
         e2e = run_e2e(fields, ops, world, args)
 
     heat = None
-    if rank == 0 and not args.no_heat:
+    if world == 1 and not args.no_heat:  # a single-GPU workload (replicas only): not run beside other ranks
         heat = run_heat()
         if not args.no_cpu:
             heat["cpu_baseline"] = cpu_heat_sample()
     ldc = None
-    if rank == 0 and not args.no_ldc:
+    if world == 1 and not args.no_ldc:  # a single-GPU workload (replicas only): not run beside other ranks
         ldc = run_ldc()
         if not args.no_cpu:
             ldc["cpu_baseline"] = cpu_ldc_sample()
     wave = None
-    if rank == 0 and not args.no_wave:
+    if world == 1 and not args.no_wave:  # a single-GPU workload (replicas only): not run beside other ranks
         wave = run_wave()
     batched = None
-    if rank == 0 and not args.no_batched:
+    if world == 1 and not args.no_batched:  # a single-GPU workload (replicas only): not run beside other ranks
         batched = run_batched(tune=not args.no_tune)
         if not args.no_cpu:
             batched["cpu_baseline"] = cpu_batched_sample()
@@ -425,6 +439,7 @@ def run_ours(args):
             "dtype": "f32", "data": "synthetic (standard normal, seeded)",
             "config": sweep_config(world),
             "roofline": roofline, "kernels": kern,
+            "kernels_isolated": {n: dict(v, frac=round(v["achieved_gbs"] / peak, 4)) for n, v in iso.items()},
             "fast_mode": {"value": world * cells * len(ops) / (fast_ms_step / 1000.0), "unit": UNIT,
                           "kernels": kern_fast,
                           "note": "PDE_MODE_FAST arithmetic (weights folded, FMA); the headline value is the "
