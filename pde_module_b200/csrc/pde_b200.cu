@@ -153,7 +153,7 @@ int launch_candidate(int cand, const float* in, float* out, const Geo& G, const 
     switch (cand) {
       case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
-      default: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 5, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 1, 64, 32, 8, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
     }
   } else if constexpr (OP == OP_LAP) {
     switch (cand) {
