@@ -265,6 +265,33 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
                     const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
                     const PdeLDCParams* params, int32_t nsteps, void* stream);
 
+/* One phase of a fractional step on a slab of the cavity: the rows
+ * [x_offset, x_offset + grid->shape[0]) of a domain of x_global rows (grid
+ * describes the slab's arrays; the other extents, ghost cells and dx are the
+ * domain's).  Results are written on the owned rows [own_lo, own_hi) only; rows
+ * beyond them are halo rows a host fills from the neighbouring slabs between
+ * phases (pde_module_b200.distributed).  Halo rows needed on a cut side
+ * (own_lo > 0, own_hi < x_global): 1 for PREDICT, DIVERGENCE (u_star) and
+ * PROJECT (u_star, p_in); nsweeps + 1 for JACOBI (p_in and rhs), which runs
+ * nsweeps sweeps from p_in into p_out (distinct) and, when `last` is set and
+ * resid is not NULL, adds the sum of squared updates of its owned cells to *resid.
+ * With one slab holding every row the phases compose pde_ldc_rollout's step,
+ * bit for bit. */
+typedef struct PdeSlab {
+  int64_t x_global;   /* rows of the whole domain, ghosts included          */
+  int64_t x_offset;   /* global row of the arrays' first row                */
+  int64_t own_lo;     /* first owned global row                             */
+  int64_t own_hi;     /* one past the last owned global row                 */
+} PdeSlab;
+#define PDE_LDC_PREDICT    0
+#define PDE_LDC_DIVERGENCE 1
+#define PDE_LDC_JACOBI     2
+#define PDE_LDC_PROJECT    3
+int pde_ldc_slab_step(int32_t phase, float* u, float* u_star, const float* p_in, float* p_out, float* rhs,
+                      float* resid, const PdeGrid* grid, const PdeSlab* slab, const PdeBCRules* u_rules,
+                      const PdeBCRules* p_rules, const PdeLDCParams* params, int32_t nsweeps, int32_t last,
+                      void* stream);
+
 /* ---- differentiable 2D wave equation (new; the reference's wave examples step a
  * first-order (u, v) pair with forward Euler, tests/FDM/test_WaveStanding.py:71-76) ----
  * State on the cells strictly inside the Dirichlet node ring (nodes and ghosts 0),

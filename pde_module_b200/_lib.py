@@ -39,6 +39,10 @@ PDE_BC_FUNC_RAMP = 1
 PDE_FUSED_MAX_COMP = 4
 PDE_MAX_GROUPS = 16
 PDE_NOALLOC_MAX_FLOATS = 1 << 22
+PDE_LDC_PREDICT = 0
+PDE_LDC_DIVERGENCE = 1
+PDE_LDC_JACOBI = 2
+PDE_LDC_PROJECT = 3
 PDE_BATCH_HEAT = 0
 PDE_BATCH_WAVE = 1
 FACE_BITS = {"-X": 1 << 0, "+X": 1 << 1, "-Y": 1 << 2, "+Y": 1 << 3, "-Z": 1 << 4, "+Z": 1 << 5}
@@ -86,6 +90,10 @@ class PdeBatchPlan(C.Structure):
                 ("rules", PdeBCRules)]
 
 
+class PdeSlab(C.Structure):
+    _fields_ = [("x_global", C.c_int64), ("x_offset", C.c_int64), ("own_lo", C.c_int64), ("own_hi", C.c_int64)]
+
+
 class PdeError(RuntimeError):
     """A C-ABI call returned a negative status."""
 
@@ -122,6 +130,10 @@ _SIGS = {
     "pde_ldc_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.POINTER(PdeBCRules),
                                   C.POINTER(PdeLDCParams), C.c_int32, C.c_void_p]),
+    "pde_ldc_slab_step": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.POINTER(PdeGrid), C.POINTER(PdeSlab), C.POINTER(PdeBCRules),
+                                    C.POINTER(PdeBCRules), C.POINTER(PdeLDCParams), C.c_int32, C.c_int32,
+                                    C.c_void_p]),
     "pde_wave_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_int64, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
                                    C.POINTER(PdeGrid), C.c_void_p]),

@@ -23,7 +23,8 @@ struct LdcConst {
 };
 
 // The three pointwise kernels run one thread per cell on a 2D grid (row =
-// blockIdx.y).  A cell whose neighbours are all at least one cell inside the
+// row0 + blockIdx.y; a slab of a larger domain passes its first owned row and
+// pointers shifted so that global row indices address its local rows).  A cell whose neighbours are all at least one cell inside the
 // node ring ("deep": x, y in [g+2, n-g-3]) reads raw values; the others go
 // through bc_eval2d, which returns the boundary-filled value of any cell.
 __device__ __forceinline__ bool ldc_deep(const Geo& G, int i, int j) {
@@ -84,8 +85,8 @@ __device__ __forceinline__ void ldc_predict_cell(const Get& at, int i, int j, co
 }
 
 __global__ void __launch_bounds__(256) ldc_predictor_kernel(const float* __restrict__ u, float* __restrict__ us,
-                                                             Geo G, const PdeBCRules Ru, LdcConst K) {
-  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+                                                             Geo G, const PdeBCRules Ru, LdcConst K, int row0) {
+  const int i = row0 + (int)blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (int)G.n[1]) return;
   const int n1 = (int)G.n[1];
   const int cell = i * n1 + j;
@@ -114,8 +115,8 @@ __device__ __forceinline__ float ldc_div_cell(const Get& at, int i, int j, const
 }
 
 __global__ void __launch_bounds__(256) ldc_divergence_kernel(const float* __restrict__ us, float* __restrict__ rhs,
-                                                              Geo G, const PdeBCRules Ru, LdcConst K) {
-  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+                                                              Geo G, const PdeBCRules Ru, LdcConst K, int row0) {
+  const int i = row0 + (int)blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (int)G.n[1]) return;
   const int n1 = (int)G.n[1];
   const int cell = i * n1 + j;
@@ -143,8 +144,8 @@ __device__ __forceinline__ void ldc_project_cell(const GetU& au, const GetP& ap,
 
 __global__ void __launch_bounds__(256) ldc_project_kernel(const float* __restrict__ us, const float* __restrict__ p,
                                                            float* __restrict__ u, Geo G, const PdeBCRules Ru,
-                                                           const PdeBCRules Rp, LdcConst K) {
-  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+                                                           const PdeBCRules Rp, LdcConst K, int row0) {
+  const int i = row0 + (int)blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= (int)G.n[1]) return;
   const int n1 = (int)G.n[1];
   const int cell = i * n1 + j;
@@ -167,7 +168,9 @@ __global__ void __launch_bounds__(256) ldc_project_kernel(const float* __restric
 // On the pass's last sweep the squared update of the tile's stencil cells is
 // reduced (warp shuffles, then one atomic per block) into *resid.
 struct J2Params {
-  int X, Y, g;
+  int X, Y, g;            // X: rows of the whole domain (a slab's arrays are addressed by global row)
+  int own_lo, own_hi;     // rows whose results this launch writes
+  int held_lo, held_hi;   // rows the arrays hold (owned rows plus halo rows on a slab's cut sides)
   int k;
   int TBX, TBY, tiles_y;
   int RXM, RYM;
@@ -180,9 +183,9 @@ __global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restric
                                                            const J2Params P, const PdeBCRules Rp) {
   extern __shared__ __align__(16) float sm[];
   const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
-  const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
+  const int bx0 = P.own_lo + tx * P.TBX, by0 = ty * P.TBY;
   const int H = P.k + 1;
-  const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, P.X);
+  const int rx0 = max(bx0 - H, P.held_lo), rx1 = min(bx0 + P.TBX + H, P.held_hi);
   const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
   const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
   const int cap = P.RXM * P.RYM;
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restric
   const int dq = nt / SW, dr = nt - dq * SW;
   // the tile in rectangle coordinates (residual cells)
   const int tx0 = bx0 - rx0 - sx0, ty0 = by0 - ry0 - sy0;
-  const int tw = min(bx0 + P.TBX, P.X) - bx0, th = min(by0 + P.TBY, P.Y) - by0;
+  const int tw = min(bx0 + P.TBX, P.own_hi) - bx0, th = min(by0 + P.TBY, P.Y) - by0;
   float sq = 0.0f;
   for (int s = 0; s < P.k; ++s) {
     bc_fill_region<1>(A, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);

@@ -914,46 +914,76 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
   return PDE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Checks and constants shared by the cavity entry points; G describes the whole domain.
+int ldc_setup(const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules, const PdeLDCParams* prm,
+              Geo* G, LdcConst* K) {
+  if (!grid || !u_rules || !p_rules || !prm) return PDE_ERR_ARG;
+  if (u_rules->ncomp != 2 || p_rules->ncomp != 1 || u_rules->has_ramp || p_rules->has_ramp) return PDE_ERR_ARG;
+  if (prm->jacobi_iters < 0 || prm->jacobi_per_pass < 0) return PDE_ERR_ARG;
+  if (!make_geo(grid, G)) return PDE_ERR_SHAPE;
+  if (G->ndims != 2 || G->n[2] != 1 || grid->order != 2) return PDE_ERR_UNSUPPORTED;
+  if (G->g < 1) return PDE_ERR_GHOST;
+  if (G->n[0] * G->n[1] >= (1LL << 30) || G->n[0] > 65535) return PDE_ERR_TOO_LARGE;  // 32-bit cells, grid rows
+  const Weights WL = lap_weights(2, grid->dx), WD = d1_weights(2, grid->dx);
+  for (int t = 0; t < 3; ++t) { K->wl[t] = WL.w[t]; K->wd[t] = WD.w[t]; }
+  K->nu = prm->nu;
+  K->dt = prm->dt;
+  K->inv_dt = (float)(1.0 / (double)prm->dt);
+  K->h2 = (float)(grid->dx * grid->dx);
+  return PDE_OK;
+}
+
+// Jacobi launch geometry for k sweeps per pass over owned rows [own_lo, own_hi)
+// of arrays holding rows [held_lo, held_hi) of a domain of G.n[0] rows.
+int jacobi_setup(const Geo& G, float h2, int k, int own_lo, int own_hi, int held_lo, int held_hi, J2Params* JP,
+                 int* tiles, size_t* smem) {
+  JP->X = (int)G.n[0]; JP->Y = (int)G.n[1]; JP->g = G.g;
+  JP->own_lo = own_lo; JP->own_hi = own_hi; JP->held_lo = held_lo; JP->held_hi = held_hi;
+  pick_tile_2d(JP->X, JP->Y, &JP->TBX, &JP->TBY);
+  JP->tiles_y = (JP->Y + JP->TBY - 1) / JP->TBY;
+  JP->RXM = JP->TBX + 2 * (k + 1);
+  JP->RYM = JP->TBY + 2 * (k + 1);
+  JP->h2 = h2;
+  *tiles = ((own_hi - own_lo + JP->TBX - 1) / JP->TBX) * JP->tiles_y;
+  *smem = (size_t)3 * JP->RXM * JP->RYM * sizeof(float);
+  if (*smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  if (cudaFuncSetAttribute(jacobi2d_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) != cudaSuccess)
+    return PDE_ERR_CUDA;
+  return PDE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid, const PdeGrid* grid,
                     const PdeBCRules* u_rules, const PdeBCRules* p_rules, const PdeLDCParams* prm, int32_t nsteps,
                     void* stream) {
-  if (!u || !p || !u_star || !p_tmp || !rhs || !grid || !u_rules || !p_rules || !prm || nsteps < 0)
-    return PDE_ERR_ARG;
-  if (u_rules->ncomp != 2 || p_rules->ncomp != 1 || u_rules->has_ramp || p_rules->has_ramp) return PDE_ERR_ARG;
-  if (prm->jacobi_iters < 0 || prm->jacobi_per_pass < 0) return PDE_ERR_ARG;
+  if (!u || !p || !u_star || !p_tmp || !rhs || nsteps < 0) return PDE_ERR_ARG;
   Geo G;
-  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
-  if (G.ndims != 2 || G.n[2] != 1 || grid->order != 2) return PDE_ERR_UNSUPPORTED;
-  if (G.g < 1) return PDE_ERR_GHOST;
-  cudaStream_t st = as_stream(stream);
-  const Weights WL = lap_weights(2, grid->dx), WD = d1_weights(2, grid->dx);
   LdcConst K;
-  for (int t = 0; t < 3; ++t) { K.wl[t] = WL.w[t]; K.wd[t] = WD.w[t]; }
-  K.nu = prm->nu;
-  K.dt = prm->dt;
-  K.inv_dt = (float)(1.0 / (double)prm->dt);
-  K.h2 = (float)(grid->dx * grid->dx);
+  int rc = ldc_setup(grid, u_rules, p_rules, prm, &G, &K);
+  if (rc) return rc;
+  cudaStream_t st = as_stream(stream);
   const int64_t cells = G.n[0] * G.n[1];
-  if (cells >= (1LL << 30) || G.n[0] > 65535) return PDE_ERR_TOO_LARGE;  // 32-bit cell indices, grid rows
-  const dim3 grid2((unsigned)((G.n[1] + 255) / 256), (unsigned)G.n[0]);
+  const int X = (int)G.n[0];
+  const dim3 grid2((unsigned)((G.n[1] + 255) / 256), (unsigned)X);
   if (resid && nsteps > 0) PDE_CUDA_CHECK(cudaMemsetAsync(resid, 0, sizeof(float) * nsteps, st));
   const int iters = prm->jacobi_iters;
   int k = prm->jacobi_per_pass > 0 ? prm->jacobi_per_pass : 10;
   if (k > iters && iters > 0) k = iters;
   J2Params JP;
-  JP.X = (int)G.n[0]; JP.Y = (int)G.n[1]; JP.g = G.g;
-  pick_tile_2d(JP.X, JP.Y, &JP.TBX, &JP.TBY);
-  JP.tiles_y = (JP.Y + JP.TBY - 1) / JP.TBY;
-  JP.RXM = JP.TBX + 2 * (k + 1);
-  JP.RYM = JP.TBY + 2 * (k + 1);
-  JP.h2 = K.h2;
-  const int jtiles = ((JP.X + JP.TBX - 1) / JP.TBX) * JP.tiles_y;
-  const size_t jsmem = (size_t)3 * JP.RXM * JP.RYM * sizeof(float);
-  if (jsmem > 227 * 1024) return PDE_ERR_TOO_LARGE;
-  PDE_CUDA_CHECK(cudaFuncSetAttribute(jacobi2d_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)jsmem));
+  int jtiles;
+  size_t jsmem;
+  rc = jacobi_setup(G, K.h2, k, 0, X, 0, X, &JP, &jtiles, &jsmem);
+  if (rc) return rc;
   for (int step = 0; step < nsteps; ++step) {
-    ldc_predictor_kernel<<<grid2, 256, 0, st>>>(u, u_star, G, *u_rules, K);
-    ldc_divergence_kernel<<<grid2, 256, 0, st>>>(u_star, rhs, G, *u_rules, K);
+    ldc_predictor_kernel<<<grid2, 256, 0, st>>>(u, u_star, G, *u_rules, K, 0);
+    ldc_divergence_kernel<<<grid2, 256, 0, st>>>(u_star, rhs, G, *u_rules, K, 0);
     float* src = p;
     float* dst = p_tmp;
     for (int done = 0; done < iters;) {
@@ -966,11 +996,78 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
       dst = t;
     }
     if (src != p) PDE_CUDA_CHECK(cudaMemcpyAsync(p, src, sizeof(float) * cells, cudaMemcpyDeviceToDevice, st));
-    ldc_project_kernel<<<grid2, 256, 0, st>>>(u_star, p, u, G, *u_rules, *p_rules, K);
-    const int rc = launch_status();
+    ldc_project_kernel<<<grid2, 256, 0, st>>>(u_star, p, u, G, *u_rules, *p_rules, K, 0);
+    rc = launch_status();
     if (rc) return rc;
   }
   return PDE_OK;
+}
+
+int pde_ldc_slab_step(int32_t phase, float* u, float* u_star, const float* p_in, float* p_out, float* rhs,
+                      float* resid, const PdeGrid* grid, const PdeSlab* slab, const PdeBCRules* u_rules,
+                      const PdeBCRules* p_rules, const PdeLDCParams* prm, int32_t nsweeps, int32_t last,
+                      void* stream) {
+  if (!grid || !slab) return PDE_ERR_ARG;
+  // the whole domain's geometry; the arrays hold rows [x_offset, x_offset + grid->shape[0])
+  PdeGrid whole = *grid;
+  whole.shape[0] = slab->x_global;
+  Geo G;
+  LdcConst K;
+  int rc = ldc_setup(&whole, u_rules, p_rules, prm, &G, &K);
+  if (rc) return rc;
+  const int64_t Xg = slab->x_global, off = slab->x_offset, nloc = grid->shape[0];
+  const int64_t lo = slab->own_lo, hi = slab->own_hi;
+  if (grid->shape[1] != whole.shape[1] || off < 0 || nloc < 1 || off + nloc > Xg || lo < off || hi > off + nloc ||
+      lo >= hi)
+    return PDE_ERR_SHAPE;
+  const int64_t Y = G.n[1];
+  cudaStream_t st = as_stream(stream);
+  // pointers addressed by global row: local row r is global row off + r
+  auto gl = [&](const float* q, int ncomp) { return q ? q - off * Y * ncomp : nullptr; };
+  const dim3 grid2((unsigned)((Y + 255) / 256), (unsigned)(hi - lo));
+  // rows one beyond the owned range on a cut side must be held (halo)
+  const bool cut_lo = lo > 0, cut_hi = hi < Xg;
+  // a ghost row's fill reads the row two steps inward: a slab with a physical
+  // side and a cut side must own rows beyond that partner
+  if ((!cut_lo && cut_hi && hi < G.g + 2) || (!cut_hi && cut_lo && lo > Xg - G.g - 2)) return PDE_ERR_SHAPE;
+  if (phase == PDE_LDC_PREDICT || phase == PDE_LDC_DIVERGENCE || phase == PDE_LDC_PROJECT) {
+    if ((cut_lo && lo - 1 < off) || (cut_hi && hi + 1 > off + nloc)) return PDE_ERR_SHAPE;
+  }
+  switch (phase) {
+    case PDE_LDC_PREDICT:
+      if (!u || !u_star) return PDE_ERR_ARG;
+      ldc_predictor_kernel<<<grid2, 256, 0, st>>>(gl(u, 2), const_cast<float*>(gl(u_star, 2)), G, *u_rules, K,
+                                                  (int)lo);
+      break;
+    case PDE_LDC_DIVERGENCE:
+      if (!u_star || !rhs) return PDE_ERR_ARG;
+      ldc_divergence_kernel<<<grid2, 256, 0, st>>>(gl(u_star, 2), const_cast<float*>(gl(rhs, 1)), G, *u_rules, K,
+                                                   (int)lo);
+      break;
+    case PDE_LDC_PROJECT:
+      if (!u || !u_star || !p_in) return PDE_ERR_ARG;
+      ldc_project_kernel<<<grid2, 256, 0, st>>>(gl(u_star, 2), gl(p_in, 1), const_cast<float*>(gl(u, 2)), G,
+                                                *u_rules, *p_rules, K, (int)lo);
+      break;
+    case PDE_LDC_JACOBI: {
+      if (!p_in || !p_out || !rhs || nsweeps < 1 || p_in == p_out) return PDE_ERR_ARG;
+      // k sweeps invalidate k + 1 rows inward from a cut side of the held rows
+      if ((cut_lo && lo - (nsweeps + 1) < off) || (cut_hi && hi + nsweeps + 1 > off + nloc)) return PDE_ERR_SHAPE;
+      J2Params JP;
+      int jtiles;
+      size_t jsmem;
+      rc = jacobi_setup(G, K.h2, nsweeps, (int)lo, (int)hi, (int)off, (int)(off + nloc), &JP, &jtiles, &jsmem);
+      if (rc) return rc;
+      JP.k = nsweeps;
+      JP.last = last ? 1 : 0;
+      jacobi2d_tb_kernel<<<jtiles, 256, jsmem, st>>>(gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1),
+                                                     resid, JP, *p_rules);
+      break;
+    }
+    default:
+      return PDE_ERR_ARG;
+  }
+  return launch_status();
 }
 
 }  // extern "C"

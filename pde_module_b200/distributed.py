@@ -77,3 +77,15 @@ def exchange_slab_halos(field: torch.Tensor, ghost: int, periodic: bool = True, 
         field[0:g].copy_(recv_lo)
     if has_right:
         field[n - g:n].copy_(recv_hi)
+
+
+def exchange_local_slabs(fields, halo: int) -> None:
+    """``exchange_slab_halos`` (not periodic) for several slabs held by one process:
+    fields[r] is slab r's array (rows ordered along X, ``halo`` rows beyond the owned
+    block on each cut side); each slab's halo rows take its neighbours' owned rows."""
+    h = int(halo)
+    for left, right in zip(fields[:-1], fields[1:]):
+        lo_send = right[h:2 * h].clone()
+        hi_send = left[left.shape[0] - 2 * h:left.shape[0] - h].clone()
+        left[left.shape[0] - h:].copy_(lo_send)
+        right[:h].copy_(hi_send)

@@ -73,3 +73,143 @@ class FractionalStepLDC:
                                     C.byref(self.u_bc.rules()), C.byref(self.p_bc.rules()), C.byref(self.params),
                                     int(nsteps), C.c_void_p(stream_ptr(self.u))), "pde_ldc_rollout")
         return self.u, self.p
+
+
+# ---- the cavity split into slabs along X (one per GPU) ----------------------------
+def slab_rows(x_global: int, world: int, halo: int, ghost: int = 1) -> list[tuple[int, int, int, int]]:
+    """(own_lo, own_hi, held_lo, held_hi) of each of `world` slabs: contiguous blocks of
+    the domain's rows (ghosts included) and `halo` more rows on each cut side."""
+    out = []
+    for r in range(world):
+        lo, hi = r * x_global // world, (r + 1) * x_global // world
+        out.append((lo, hi, max(lo - halo, 0), min(hi + halo, x_global)))
+    for r, (lo, hi, _, _) in enumerate(out):
+        if world > 1 and hi - lo < max(halo, ghost + 2):
+            raise ValueError(f"slab {r} owns {hi - lo} rows: at least {max(halo, ghost + 2)} needed")
+    return out
+
+
+class LDCSlab:
+    """One slab of the cavity of FractionalStepLDC (same parameters): owned rows
+    [own_lo, own_hi) of the (n+2g)^2 domain plus halo rows on its cut sides.  Each
+    method runs one phase of a fractional step on this slab (pde_ldc_slab_step); a
+    host fills the halo rows between phases (``ldc_slab_steps``)."""
+
+    def __init__(self, rows, n: int = 1024, Re: float = 100.0, lid: float = 1.0, cfl: float = 0.2,
+                 jacobi_iters: int = 50, jacobi_per_pass: int = 0, ghost_cells: int = 1, device="cuda",
+                 dt: float | None = None) -> None:
+        from .. import _lib
+        g = int(ghost_cells)
+        self.n, self.g = int(n), g
+        self.dx = 1.0 / (n - 1)
+        self.lid = float(lid)
+        self.nu = lid * 1.0 / Re
+        self.dt = float(dt) if dt is not None else cfl * min(self.dx / max(abs(lid), 1e-30),
+                                                               self.dx * self.dx / (4.0 * self.nu))
+        self.own_lo, self.own_hi, self.held_lo, self.held_hi = (int(v) for v in rows)
+        X = n + 2 * g
+        nloc = self.held_hi - self.held_lo
+        shape = (nloc, X, 1)
+        z = lambda c: torch.zeros(shape + (c,), dtype=torch.float32, device=device)
+        self.u, self.u_star, self.p, self.p_tmp, self.rhs = z(2), z(2), z(1), z(1), z(1)
+        # boundary rules of the whole domain (face groups: the same for every slab)
+        whole_u = torch.zeros((X, X, 1, 2))
+        self.u_bc = GridBoundary(whole_u, self.dx, g)
+        self.u_bc.dirichlet_BC("ALL", 0.0)
+        self.u_bc.dirichlet_BC("+Y", self.lid, 0)
+        self.p_bc = GridBoundary(whole_u[..., :1], self.dx, g)
+        self.p_bc.vonNeumann_BC("ALL", 0.0)
+        self._u_rules, self._p_rules = self.u_bc.rules(), self.p_bc.rules()
+        self.params = PdeLDCParams(self.nu, self.dt, int(jacobi_iters), int(jacobi_per_pass))
+        self.grid = make_grid(shape, g, 2, self.dx)
+        self.slab = _lib.PdeSlab(X, self.held_lo, self.own_lo, self.own_hi)
+        self.resid = torch.zeros(1, dtype=torch.float32, device=device)
+
+    @property
+    def owned(self) -> slice:
+        """Local rows of the owned block."""
+        return slice(self.own_lo - self.held_lo, self.own_hi - self.held_lo)
+
+    def _phase(self, phase, p_in=None, p_out=None, nsweeps=0, last=False, resid=False):
+        P = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        check(lib().pde_ldc_slab_step(phase, P(self.u), P(self.u_star), P(p_in), P(p_out), P(self.rhs),
+                                      P(self.resid) if resid else None, C.byref(self.grid), C.byref(self.slab),
+                                      C.byref(self._u_rules), C.byref(self._p_rules), C.byref(self.params),
+                                      int(nsweeps), int(bool(last)), C.c_void_p(stream_ptr(self.u))),
+              "pde_ldc_slab_step")
+
+    def predict(self):
+        from .. import _lib
+        self._phase(_lib.PDE_LDC_PREDICT)
+
+    def divergence(self):
+        from .. import _lib
+        self._phase(_lib.PDE_LDC_DIVERGENCE)
+
+    def jacobi(self, nsweeps: int, last: bool, residual: bool = False):
+        """nsweeps sweeps from p into p_tmp, then the two are swapped."""
+        from .. import _lib
+        self._phase(_lib.PDE_LDC_JACOBI, self.p, self.p_tmp, nsweeps, last, residual)
+        self.p, self.p_tmp = self.p_tmp, self.p
+
+    def project(self):
+        from .. import _lib
+        self._phase(_lib.PDE_LDC_PROJECT, self.p)
+
+
+def ldc_slab_steps(slabs, nsteps: int, exchange, residuals: bool = False) -> None:
+    """Advance the slabs of one cavity nsteps fractional steps.  ``exchange(fields)``
+    fills the halo rows of the listed fields (one per slab, in slab order) from the
+    neighbouring slabs: ``exchange_slab_halos`` across ranks, ``exchange_local_slabs``
+    for several slabs in one process.  With residuals, each slab's ``resid`` holds the
+    sum of squared pressure updates of its owned cells over the last step's last sweep."""
+    s0 = slabs[0]
+    iters = s0.params.jacobi_iters
+    k = s0.params.jacobi_per_pass or 10
+    for _ in range(nsteps):
+        if residuals:
+            for s in slabs:
+                s.resid.zero_()
+        exchange([s.u for s in slabs])
+        for s in slabs:
+            s.predict()
+        exchange([s.u_star for s in slabs])
+        for s in slabs:
+            s.divergence()
+        exchange([s.rhs for s in slabs])
+        done = 0
+        while done < iters:
+            kk = min(k, iters - done)
+            done += kk
+            exchange([s.p for s in slabs])
+            for s in slabs:
+                s.jacobi(kk, done == iters, residuals)
+        exchange([s.p for s in slabs])
+        for s in slabs:
+            s.project()
+
+
+class SlabFractionalStepLDC:
+    """FractionalStepLDC split across the ranks of a process group (one slab of rows
+    per rank, one GPU per rank): halo rows are exchanged between phases with
+    point-to-point send/recv (NCCL over NVLink), the residual summed with all_reduce."""
+
+    def __init__(self, n: int = 1024, Re: float = 100.0, jacobi_iters: int = 50, jacobi_per_pass: int = 0,
+                 group=None, device="cuda", **kw) -> None:
+        import torch.distributed as dist
+        from ..distributed import exchange_slab_halos
+        self.group = group
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+        k = jacobi_per_pass or 10
+        self.halo = k + 1
+        rows = slab_rows(n + 2, world, self.halo)[rank]
+        self.slab = LDCSlab(rows, n=n, Re=Re, jacobi_iters=jacobi_iters, jacobi_per_pass=jacobi_per_pass,
+                            device=device, **kw)
+        self._exchange = lambda fields: exchange_slab_halos(fields[0], self.halo, periodic=False, group=group)
+
+    def step(self, nsteps: int = 1, residuals: bool = False):
+        import torch.distributed as dist
+        ldc_slab_steps([self.slab], nsteps, self._exchange, residuals)
+        if residuals:
+            dist.all_reduce(self.slab.resid, group=self.group)
+        return self.slab.u, self.slab.p

@@ -138,3 +138,20 @@ def test_distributed_batch_equals_single_process():
         dx = 1.0 / max(sx, sy)
         groups = fdm.standard_groups((sx + 2, sy + 2, 1), 1, [("ALL", 1, 0.0, (0,))])
         assert np.array_equal(merged[i], fdm.heat_rollout(u0, groups, dx, 1, 0.5, 0.2 * dx * dx / 0.5, 9))
+
+
+def test_slab_rows_and_local_exchange():
+    from pde_module_b200.time_step.fractional_step import slab_rows
+    from pde_module_b200.distributed import exchange_local_slabs
+    rows = slab_rows(50, 3, 4)
+    assert [r[0] for r in rows] == [0, 16, 33] and rows[-1][1] == 50
+    assert all(hl == max(lo - 4, 0) and hh == min(hi + 4, 50) for lo, hi, hl, hh in rows)
+    with pytest.raises(ValueError):
+        slab_rows(20, 4, 6)  # 5 rows per slab < halo
+    glob = torch.arange(50 * 3, dtype=torch.float32).reshape(50, 3)
+    fields = [torch.full((hh - hl, 3), -1.0) for lo, hi, hl, hh in rows]
+    for f, (lo, hi, hl, hh) in zip(fields, rows):
+        f[lo - hl:hi - hl] = glob[lo:hi]
+    exchange_local_slabs(fields, 4)
+    for f, (lo, hi, hl, hh) in zip(fields, rows):
+        assert torch.equal(f, glob[hl:hh])

@@ -41,3 +41,22 @@ def test_ldc_lid_drives_a_vortex():
     assert abs(col[-1] - 1.0) < 1e-2              # lid node (reset by the next step's boundary fill)
     assert col[-3] > 0.1                           # fluid dragged by the lid near the top
     assert col[len(col) // 4] < 0.0                # return flow in the lower half
+
+
+@pytest.mark.parametrize("n,slabs,iters,k,steps", [(60, 2, 23, 5, 3), (75, 3, 12, 4, 2), (40, 1, 10, 3, 2)])
+def test_slabs_match_whole_domain(n, slabs, iters, k, steps):
+    """The cavity split into slabs along X (halo rows filled between phases, as the
+    multi-GPU path does across ranks) is bit-identical to the whole-domain rollout."""
+    from pde_module_b200.time_step.fractional_step import LDCSlab, slab_rows, ldc_slab_steps
+    from pde_module_b200.distributed import exchange_local_slabs
+    whole = P.FractionalStepLDC(n=n, Re=100.0, jacobi_iters=iters, jacobi_per_pass=k)
+    whole.step(steps)
+    halo = k + 1
+    parts = [LDCSlab(r, n=n, Re=100.0, jacobi_iters=iters, jacobi_per_pass=k)
+             for r in slab_rows(n + 2, slabs, halo)]
+    ldc_slab_steps(parts, steps, lambda fields: exchange_local_slabs(fields, halo))
+    torch.cuda.synchronize()
+    for s in parts:
+        rows = slice(s.own_lo, s.own_hi)
+        assert torch.equal(s.u[s.owned], whole.u[rows]), (s.own_lo, s.own_hi)
+        assert torch.equal(s.p[s.owned], whole.p[rows]), (s.own_lo, s.own_hi)
