@@ -1,5 +1,5 @@
 from .forwardEuler import ForwardEuler
 from .heat import HeatRollout, HeatSolver, heat_rollout
-from .fractional_step import FractionalStepLDC
+from .fractional_step import FractionalStepLDC, SlabFractionalStepLDC
 from .wave import WaveSolver, wave_rollout
 from .batched import BatchedHeatRollout, BatchedWaveRollout
