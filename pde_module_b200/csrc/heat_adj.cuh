@@ -219,7 +219,51 @@ __global__ void __launch_bounds__(1024) heat2d_adj_kernel(const float* __restric
   __syncthreads();
   const int dq = (int)blockDim.x / RY, dr = (int)blockDim.x - dq * RY;
   const int lxs = (int)threadIdx.x / RY, lys = (int)threadIdx.x - lxs * RY;
-  for (int s = 0; s < P.k; ++s) {
+  // A region without ghost, node or partner cells (x, y in [g+2, n-g-3] throughout)
+  // has B^T = identity and only stencil cells: a step is one pass, mu written as the
+  // new lam in place (a cell reads only its own lam) and the next z into a second
+  // buffer (M, not otherwise needed here).  The same values as the two-pass step.
+  const bool interior = rx0 > g + 1 && rx0 + RX < X - g - 2 && ry0 > g + 1 && ry0 + RY < Y - g - 2;
+  float* Zc = Z;
+  float* Zn = M;
+  for (int s = 0; s < P.k && interior; ++s) {
+    if (s + 1 < P.k) fetch_S(s + 1, (s + 1) & 1);  // its slot was last read in step s-1
+    const float* Sg = GL + (s & 1) * OT;
+    int lx = lxs, ly = lys;
+    for (int i = threadIdx.x; i < RC; i += blockDim.x) {
+      float acc = 0.0f;
+#pragma unroll
+      for (int t = 0; t < 2 * R + 1; ++t) {
+        const int nx = lx + t - R;
+        const float zv = (nx >= 0 && nx < RX) ? Zc[i + (t - R) * RY] : 0.0f;
+        acc = add(acc, mul(P.w[t], zv));
+      }
+#pragma unroll
+      for (int t = 0; t < 2 * R + 1; ++t) {
+        const int ny = ly + t - R;
+        const float zv = (ny >= 0 && ny < RY) ? Zc[i + (t - R)] : 0.0f;
+        acc = add(acc, mul(P.w[t], zv));
+      }
+      const float l = Lm[i];
+      const float m = add(l, acc);
+      const int x = rx0 + lx, y = ry0 + ly;
+      if (x >= bx0 && x < ox1 && y >= by0 && y < oy1) {
+        const int gi = (x - bx0) * OY + (y - by0);
+        GA[gi] = add(GA[gi], mul(l, mul(dt, Sg[gi])));
+      }
+      Lm[i] = m;
+      Zn[i] = mul(dt, mul(AL[i], m));
+      lx += dq;
+      ly += dr;
+      if (ly >= RY) { ly -= RY; ++lx; }
+    }
+    cp_async_wait_all();  // this thread's copies of the next step's S; the barrier publishes them
+    __syncthreads();
+    float* t = Zc;
+    Zc = Zn;
+    Zn = t;
+  }
+  for (int s = 0; s < P.k && !interior; ++s) {
     if (s + 1 < P.k) fetch_S(s + 1, (s + 1) & 1);  // its slot was last read in step s-1
     const float* Sg = GL + (s & 1) * OT;
     // mu = lam + L^T(z); the gradient term of step n on the tile
