@@ -32,6 +32,32 @@ int sm_count() {
 
 int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ERR_CUDA; }
 
+// A 2D tile count just above m x SMs (m = 1, 2) leaves a short tail wave in which
+// a few SMs run a second tile while the rest wait: enlarge the tiles slightly
+// (at most two fewer tiles per axis, sides up to 256) so the count drops to m x SMs.
+void balance_tiles(int X, int Y, int* tbx, int* tby) {
+  const long long sms = sm_count();
+  const long long nx = (X + *tbx - 1) / *tbx, ny = (Y + *tby - 1) / *tby;
+  for (long long m = 1; m <= 2; ++m) {
+    const long long cap = m * sms;
+    if (nx * ny <= cap) return;
+    if (nx * ny * 4 > cap * 5) continue;
+    long long bx = 0, by = 0;
+    for (long long ax = nx - 2; ax <= nx; ++ax)
+      for (long long ay = ny - 2; ay <= ny; ++ay)
+        if (ax >= 1 && ay >= 1 && ax * ay <= cap && ax * ay > bx * by) {
+          bx = ax;
+          by = ay;
+        }
+    if (bx == 0) return;
+    const int tx = (int)((X + bx - 1) / bx), ty = (int)((Y + by - 1) / by);
+    if (tx > 256 || ty > 256) return;
+    *tbx = tx;
+    *tby = ty;
+    return;
+  }
+}
+
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
 // ---- 3D streaming dispatch -------------------------------------------------
@@ -537,9 +563,9 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
 
 namespace {
 
-// Output tile of the temporally blocked 2D kernels (differentiable heat, wave):
-// the largest of 32x64, 32x32, 16x32 that still gives every SM a tile, unless
-// pde_set_launch_2d fixed one.
+// Output tile of the temporally blocked 2D kernels (differentiable heat, wave,
+// cavity): the largest of 32x64, 32x32, 16x32 that still gives every SM a tile,
+// balanced against the SM count, unless pde_set_launch_2d fixed one.
 int g_tile2d[2] = {0, 0};
 int g_threads2d = 0;
 
@@ -548,8 +574,8 @@ int g_threads2d = 0;
 int pick_threads_2d(long long tiles) {
   if (g_threads2d > 0) return g_threads2d;
   const double per_sm = (double)tiles / sm_count();
-  if (per_sm <= 1.1) return 1024;
-  if (per_sm <= 2.2) return 512;
+  if (per_sm <= 1.0) return 1024;
+  if (per_sm <= 2.0) return 512;
   return 256;
 }
 
@@ -565,6 +591,7 @@ void pick_tile_2d(int X, int Y, int* tbx, int* tby) {
     if (tiles >= sm_count() || c == 2) {
       *tbx = cand[c][0];
       *tby = cand[c][1];
+      balance_tiles(X, Y, tbx, tby);
       return;
     }
   }
