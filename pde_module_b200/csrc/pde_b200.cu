@@ -759,6 +759,15 @@ bool wave_setup(const PdeGrid* grid, int steps_per_pass, int nsteps, Geo* G, Wav
   return *smem <= 227 * 1024;
 }
 
+// Register cell lists of the wave adjoint kernels: the region capacity bounds
+// every block's rectangle, so MAXC cells per thread cover it; 0 = the general
+// loop (rectangles beyond 8 cells per thread).
+int wave_cells_per_thread(int rc, int threads) {
+  if (rc <= 4 * threads) return 4;
+  if (rc <= 8 * threads) return 8;
+  return 0;
+}
+
 }  // namespace
 
 int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, float* out_prev, float* out_cur,
@@ -848,9 +857,11 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
   Pa.gK = grad_K;
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)Pa.cells;
-  PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_pair_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((Pa.X + Pa.TBX - 1) / Pa.TBX) * Pa.tiles_y;
   const int threads = pick_threads_2d(tiles);
+  const int cpt = wave_cells_per_thread(Pa.RC, threads);
+  auto kern = cpt == 4 ? wave_pair_tb_kernel<4> : cpt == 8 ? wave_pair_tb_kernel<8> : wave_pair_tb_kernel<0>;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   float* w[6];
   for (int i = 0; i < 6; ++i) w[i] = work + (size_t)i * Pa.cells;
   // forward part: (u_prev, u_cur) -> (w0, w1) -> (w2, w3) -> (w0, w1) ...; the inputs are never written
@@ -873,7 +884,7 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
     float* fo_b = w[2 * fslot + 1];
     float* mo_a = to_out ? mu_out : w[4];
     float* mo_b = to_out ? mu_out_next : w[5];
-    wave_pair_tb_kernel<<<tiles, threads, smem, st>>>(fa, fb, fo_a, fo_b, ma, mb, mo_a, mo_b, K, Pf, Pa);
+    kern<<<tiles, threads, smem, st>>>(fa, fb, fo_a, fo_b, ma, mb, mo_a, mo_b, K, Pf, Pa);
     const int rc = launch_status();
     if (rc) return rc;
     if (Pf.k > 0) {
@@ -908,9 +919,11 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
 
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)P.cells;
-  PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_adj_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
   const int threads = pick_threads_2d(tiles);
+  const int cpt = wave_cells_per_thread(P.RC, threads);
+  auto kern = cpt == 4 ? wave_adj_tb_kernel<4> : cpt == 8 ? wave_adj_tb_kernel<8> : wave_adj_tb_kernel<0>;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int npasses = (nsteps + k - 1) / k;
   float* w0 = work;
   float* w1 = work + P.cells;
@@ -926,7 +939,7 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
     P.ntop = nsteps - 1 - done;
     float* da = to_out ? mu_out : w0;
     float* db = to_out ? mu_out_next : w1;
-    wave_adj_tb_kernel<<<tiles, threads, smem, st>>>(a, b, K, da, db, P);
+    kern<<<tiles, threads, smem, st>>>(a, b, K, da, db, P);
     const int rc = launch_status();
     if (rc) return rc;
     a = da;

@@ -79,6 +79,32 @@ struct WaveRect {
   }
 };
 
+// The rectangle cells of this thread, q = threadIdx.x + c * blockDim.x for
+// c < MAXC: the same cells in every step (the rectangle is fixed for the pass),
+// so their indices, the gradient sums of the tile cells among them and the next
+// step's L(u^n) values stay in registers.  Needs count <= MAXC * blockDim.x.
+template <int MAXC>
+struct WaveCells {
+  int ri[MAXC];  // region index; -1 past the rectangle
+  int gi[MAXC];  // array index of a tile cell; -1 for the other cells
+  __device__ WaveCells(const WaveRect& Rt, const WaveRegion& Rg, int Y) {
+    const int nt = (int)blockDim.x;
+    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
+    RectWalk wk(Rt.W, nt);
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      ri[c] = -1;
+      gi[c] = -1;
+      if ((int)threadIdx.x + c * nt < Rt.count) {
+        ri[c] = (Rt.cx0 + wk.row) * Rg.RY + Rt.cy0 + wk.col;
+        const int ox = wk.row - tx0, oy = wk.col - ty0;
+        if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) gi[c] = (Rg.bx0 + ox) * Y + Rg.by0 + oy;
+      }
+      wk.next();
+    }
+  }
+};
+
 // Load a region row-major (RX x RY) with fn(region index, array x, array y).
 template <class F>
 __device__ __forceinline__ void for_region(const WaveRegion& Rg, F fn) {
@@ -170,6 +196,10 @@ __global__ void __launch_bounds__(1024) wave_fwd_tb_kernel(const float* __restri
   });
 }
 
+// MAXC > 0: the cells of a thread in registers (WaveCells), the gradient sums
+// of its tile cells in registers and L(u^n) of the next step loaded while this
+// one computes; MAXC = 0: any rectangle size, gradient tile in shared memory.
+template <int MAXC>
 __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restrict__ m1_in,
                                                             const float* __restrict__ m2_in,
                                                             const float* __restrict__ Kf, float* __restrict__ m1_out,
@@ -189,12 +219,60 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
     sm[o0 + i] = 0.0f;
     sm[k0 + i] = 0.0f;
   });
-  for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, P.gK + gi, true); });
+  if (MAXC == 0) for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, P.gK + gi, true); });
   cp_async_wait_all();
   // K o mu^{n+1} of the cells this thread copied (its own copies are complete)
   for_region(Rg, [&](int i, int x, int y) { sm[k1 + i] = mul(sm[okk + i], sm[o1 + i]); });
   __syncthreads();
   const WaveRect Rt(P, Rg);
+  if constexpr (MAXC > 0) {
+    const WaveCells<MAXC> C(Rt, Rg, P.Y);
+    float ga[MAXC], lnext[MAXC];
+    const float* L0 = P.lsts + (size_t)P.ntop * P.cells;
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      ga[c] = C.gi[c] >= 0 ? P.gK[C.gi[c]] : 0.0f;
+      lnext[c] = C.gi[c] >= 0 ? __ldg(L0 + C.gi[c]) : 0.0f;
+    }
+    for (int s = 0; s < P.k; ++s) {
+      float ln[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) ln[c] = lnext[c];
+      if (s + 1 < P.k) {
+        const float* L1 = P.lsts + (size_t)(P.ntop - s - 1) * P.cells;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        const int i = C.ri[c];
+        if (i < 0) continue;
+        const float m1 = sm[o1 + i];
+        if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
+        const float acc = lap5s(sm, k1 + i, RY, P.w);
+        const float v = add(sub(mul(2.0f, m1), sm[o2 + i]), acc);
+        sm[o0 + i] = v;
+        sm[k0 + i] = mul(sm[okk + i], v);
+      }
+      __syncthreads();
+      const int t = o2;
+      o2 = o1;
+      o1 = o0;
+      o0 = t;
+      const int u = k1;
+      k1 = k0;
+      k0 = u;
+    }
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c)
+      if (C.gi[c] >= 0) P.gK[C.gi[c]] = ga[c];
+    for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
+      m1_out[gi] = sm[o1 + ri];
+      m2_out[gi] = sm[o2 + ri];
+    });
+    return;
+  }
   const int nt = (int)blockDim.x;
   const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
   for (int s = 0; s < P.k; ++s) {
@@ -240,6 +318,9 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
 // of both costs one barrier.  Arithmetic and per-cell operation order are
 // those of the two kernels above.  Shared memory (offsets of RC cells): forward
 // levels 0-2, adjoint levels 3-5, K o mu 6-7, K 8, then the gradient tile.
+// MAXC as in wave_adj_tb_kernel (the forward's stored Laplacians use the same
+// tile indices).
+template <int MAXC>
 __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restrict__ um_in,
                                                              const float* __restrict__ u0_in,
                                                              float* __restrict__ um_out, float* __restrict__ u0_out,
@@ -273,15 +354,97 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
       sm[k0 + i] = 0.0f;
     }
   });
-  if (adj) for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, Pa.gK + gi, true); });
+  if (adj && MAXC == 0)
+    for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, Pa.gK + gi, true); });
   cp_async_wait_all();
   if (adj) for_region(Rg, [&](int i, int x, int y) { sm[k1 + i] = mul(sm[okk + i], sm[a1 + i]); });
   __syncthreads();
   const WaveRect Rt(Pa, Rg);
-  const int nt = (int)blockDim.x;
-  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
   const int srci = (Pf.srcx >= 0 && Pf.srcx >= rx0 && Pf.srcx < rx0 + Rg.RX && Pf.srcy >= ry0 && Pf.srcy < ry0 + RY)
                        ? (Pf.srcx - rx0) * RY + (Pf.srcy - ry0) : -1;
+  if constexpr (MAXC > 0) {
+    const WaveCells<MAXC> C(Rt, Rg, Pa.Y);
+    float ga[MAXC], lnext[MAXC];
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      ga[c] = 0.0f;
+      lnext[c] = 0.0f;
+      if (adj && C.gi[c] >= 0) {
+        ga[c] = Pa.gK[C.gi[c]];
+        lnext[c] = __ldg(Pa.lsts + (size_t)Pa.ntop * Pa.cells + C.gi[c]);
+      }
+    }
+    for (int s = 0; s < H; ++s) {
+      const bool fs = s < Pf.k, as = s < Pa.k;
+      const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
+      float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
+      float ln[MAXC];
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) ln[c] = lnext[c];
+      if (s + 1 < Pa.k) {
+        const float* L1 = Pa.lsts + (size_t)(Pa.ntop - s - 1) * Pa.cells;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c)
+          if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        const int i = C.ri[c];
+        if (i < 0) continue;
+        if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+          const float lap = lap5s(sm, f0 + i, RY, Pf.w);
+          float v = sub(mul(2.0f, sm[f0 + i]), sm[fm + i]);
+          v = add(v, mul(sm[okk + i], lap));
+          if (i == srci) v = add(v, sn);
+          sm[fp + i] = v;
+          if (C.gi[c] >= 0) Ls[C.gi[c]] = lap;
+        }
+        if (as) {
+          const float m1 = sm[a1 + i];
+          if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
+          // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+          const float acc = lap5s(sm, k1 + i, RY, Pa.w);
+          const float v = add(sub(mul(2.0f, m1), sm[a2 + i]), acc);
+          sm[a0 + i] = v;
+          sm[k0 + i] = mul(sm[okk + i], v);
+        }
+      }
+      __syncthreads();
+      if (fs) {
+        const int t = fm;
+        fm = f0;
+        f0 = fp;
+        fp = t;
+      }
+      if (as) {
+        int t = a2;
+        a2 = a1;
+        a1 = a0;
+        a0 = t;
+        t = k1;
+        k1 = k0;
+        k0 = t;
+      }
+    }
+    if (adj) {
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c)
+        if (C.gi[c] >= 0) Pa.gK[C.gi[c]] = ga[c];
+    }
+    for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) {
+      if (fwd) {
+        um_out[gi] = sm[fm + ri];
+        u0_out[gi] = sm[f0 + ri];
+      }
+      if (adj) {
+        m1_out[gi] = sm[a1 + ri];
+        m2_out[gi] = sm[a2 + ri];
+      }
+    });
+    return;
+  }
+  const int nt = (int)blockDim.x;
+  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
   for (int s = 0; s < H; ++s) {
     const bool fs = s < Pf.k, as = s < Pa.k;
     const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
