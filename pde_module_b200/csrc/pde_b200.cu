@@ -793,9 +793,11 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
     P.srcy = (int)(src_cell % P.Y);
     P.src = src;
   }
-  PDE_CUDA_CHECK(cudaFuncSetAttribute(wave_fwd_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
   const int threads = pick_threads_2d(tiles);
+  const int cpt = wave_cells_per_thread(P.RC, threads);
+  auto kern = cpt == 4 ? wave_fwd_tb_kernel<4> : cpt == 8 ? wave_fwd_tb_kernel<8> : wave_fwd_tb_kernel<0>;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int npasses = (nsteps + k - 1) / k;
   float* w0 = work;
   float* w1 = work + P.cells;
@@ -810,7 +812,7 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
     P.lst = lstates ? lstates + (size_t)done * P.cells : nullptr;
     float* da = to_out ? out_prev : w0;
     float* db = to_out ? out_cur : w1;
-    wave_fwd_tb_kernel<<<tiles, threads, smem, st>>>(a, b, K, da, db, P);
+    kern<<<tiles, threads, smem, st>>>(a, b, K, da, db, P);
     const int rc = launch_status();
     if (rc) return rc;
     a = da;

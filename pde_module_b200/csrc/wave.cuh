@@ -135,7 +135,7 @@ __device__ __forceinline__ float lap5s(const float* sm, int i, int RY, const flo
 
 // k forward steps; the three levels are rotated as offsets into the one
 // shared-memory array (om: u^{n-1}, o0: u^n, op: u^{n+1}).
-template <bool STORE>
+template <bool STORE, int MAXC>
 __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRegion& Rg, float* sm, int& om,
                                                int& o0, int& op, int ok) {
   const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
@@ -143,6 +143,30 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
   const int nt = (int)blockDim.x;
   const int srci = (P.srcx >= 0 && P.srcx >= rx0 && P.srcx < rx0 + Rg.RX && P.srcy >= ry0 && P.srcy < ry0 + RY)
                        ? (P.srcx - rx0) * RY + (P.srcy - ry0) : -1;
+  if constexpr (MAXC > 0) {
+    const WaveCells<MAXC> C(Rt, Rg, P.Y);
+    for (int s = 0; s < P.k; ++s) {
+      const float sn = (srci >= 0) ? P.src[P.n0 + s] : 0.0f;
+      float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
+#pragma unroll
+      for (int c = 0; c < MAXC; ++c) {
+        const int i = C.ri[c];
+        if (i < 0) continue;
+        const float lap = lap5s(sm, o0 + i, RY, P.w);
+        float v = sub(mul(2.0f, sm[o0 + i]), sm[om + i]);
+        v = add(v, mul(sm[ok + i], lap));
+        if (i == srci) v = add(v, sn);
+        sm[op + i] = v;
+        if (STORE && C.gi[c] >= 0) Ls[C.gi[c]] = lap;
+      }
+      __syncthreads();
+      const int t = om;
+      om = o0;
+      o0 = op;
+      op = t;
+    }
+    return;
+  }
   // the tile in rectangle coordinates (for the stored Laplacians)
   const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
   for (int s = 0; s < P.k; ++s) {
@@ -170,6 +194,7 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
   }
 }
 
+template <int MAXC>
 __global__ void __launch_bounds__(1024) wave_fwd_tb_kernel(const float* __restrict__ um_in,
                                                             const float* __restrict__ u0_in,
                                                             const float* __restrict__ Kf, float* __restrict__ um_out,
@@ -188,8 +213,8 @@ __global__ void __launch_bounds__(1024) wave_fwd_tb_kernel(const float* __restri
   });
   cp_async_wait_all();
   __syncthreads();
-  if (P.lst) wave_fwd_steps<true>(P, Rg, sm, om, o0, op, ok);
-  else wave_fwd_steps<false>(P, Rg, sm, om, o0, op, ok);
+  if (P.lst) wave_fwd_steps<true, MAXC>(P, Rg, sm, om, o0, op, ok);
+  else wave_fwd_steps<false, MAXC>(P, Rg, sm, om, o0, op, ok);
   for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
     um_out[gi] = sm[om + ri];
     u0_out[gi] = sm[o0 + ri];
