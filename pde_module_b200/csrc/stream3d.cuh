@@ -69,10 +69,15 @@ struct S3Cfg {
   // MAP_PAIRS: each half (even / odd rows) is a dense [ROWS/2][W] box, 128-byte aligned
   static constexpr int HALF = ((ROWS / 2) * W + 31) & ~31;
   static constexpr int STAGE_FLOATS = (MAPK == MAP_PAIRS) ? 2 * HALF : ROWS * WP;
-  // Grad: per consumer warp, YPT rows x 32 cells x 3 outputs staged for contiguous stores
-  static constexpr int OBUF_FLOATS = (OP == OP_GRAD) ? NCW * YPT * 96 : 0;
+  // Grad: the tile's TY output rows of a plane (3 TZ floats each, placed at the
+  // row's offset within a 128-byte line: pitch 3 TZ + 32); two planes' buffers
+  // where two blocks per SM still fit, else one (and a second barrier per plane)
+  static constexpr int OROW = 3 * TZ + 32;
   // + 128: the base is rounded up to a 128-byte boundary at run time
-  static constexpr size_t SMEM = (size_t)S * STAGE_FLOATS * 4 + (size_t)2 * S * 8 + (size_t)OBUF_FLOATS * 4 + 128;
+  static constexpr size_t SMEM_BASE = (size_t)S * STAGE_FLOATS * 4 + (size_t)2 * S * 8 + 128;
+  static constexpr int OBUFS = (SMEM_BASE + (size_t)2 * TY * OROW * 4 <= 113 * 1024) ? 2 : 1;
+  static constexpr int OBUF_FLOATS = (OP == OP_GRAD) ? OBUFS * TY * OROW : 0;
+  static constexpr size_t SMEM = SMEM_BASE + (size_t)OBUF_FLOATS * 4;
   static_assert(NCONS % 32 == 0, "whole consumer warps");
   static_assert(W <= 256, "TMA box extent");
   static_assert(TY % YPT == 0, "rows per thread");
@@ -193,6 +198,10 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
     __syncwarp();
     if (warp_leader) mbar_arrive(&empty[st]);
   };
+
+  int opc = 0;  // grad: planes stored so far (selects the staging buffer)
+  const int obase = (int)((reinterpret_cast<uintptr_t>(P.out) >> 2) & 31u);  // grad: out's float offset in its line
+  const int dzr = (3 * P.Z) & 31;  // grad: line offset step from one output row to the next
 
   const int zrow = P.Z * CIN;
   const int oplane = (OP == OP_LAP) ? P.Y * zrow : P.Y * P.Z * ((OP == OP_GRAD) ? 3 : 1);
@@ -337,32 +346,51 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
         }
         release(cs);  // the centre plane is not read again
         adv(cs);
-        float* op = optr + j * oplane;
+        [[maybe_unused]] float* op = optr + j * oplane;  // this thread's first output (LAP, DIV)
         if constexpr (OP == OP_GRAD) {
-          // The warp's 32 cells of a row own 96 consecutive output floats: stage them
-          // in shared memory and store them as 3 coalesced 128-byte rows.
-          const int wl = tid & 31;
-          float* wb = obuf + (tid >> 5) * (YPT * 96);
+          // A tile row owns 3 TZ consecutive output floats (TZ / 32 warps compute
+          // it).  The consumers stage the plane's rows in shared memory, each at its
+          // global offset within a 128-byte line, meet at a named barrier, and every
+          // warp then stores whole rows as line-aligned 128-byte pieces: each store
+          // covers one line, and a row goes out as one contiguous run.  Two
+          // buffers: a buffer is rewritten two planes later, after every consumer
+          // has passed the next plane's barrier, i.e. finished reading it; one
+          // buffer: a second barrier after the stores.
+          float* ob = obuf + (C::OBUFS == 2 ? (opc & 1) * (TY * C::OROW) : 0);
+          ++opc;
+          // tile row t of this plane starts rf0 + 3 Z t floats into the array, at
+          // float (r0 + dzr t) mod 32 of a 128-byte line
+          const size_t rf0 = (((size_t)(xs + j) * P.Y + y0) * P.Z + z0) * 3;
+          const int r0 = (obase + (int)(rf0 & 31u)) & 31;
 #pragma unroll
           for (int k = 0; k < YPT; ++k) {
-            wb[k * 96 + wl * 3 + 0] = res[k][0];
-            wb[k * 96 + wl * 3 + 1] = res[k][1];
-            wb[k * 96 + wl * 3 + 2] = res[k][2];
+            const int t = row0 + k;
+            float* sr = ob + t * C::OROW + ((r0 + t * dzr) & 31) + 3 * lane;
+            sr[0] = res[k][0];
+            sr[1] = res[k][1];
+            sr[2] = res[k][2];
           }
-          __syncwarp();
-          // op points at this lane's cell (3 floats); the warp's span starts 3*wl floats earlier
-          float* ob = op - 3 * wl;
-          const int zspan = zcell - wl;  // first cell of the warp's span
+          asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
+          const int wl = tid & 31;
+          const int nf = 3 * min(TZ, P.Z - P.g - z0);  // floats of the row's interior cells
+          constexpr int NL = 3 * TZ / 32 + 1;          // lines a row can touch
+          for (int t = tid >> 5; t < TY && y0 + t < P.Y - P.g; t += C::NCW) {
+            const int r = (r0 + t * dzr) & 31;
+            const int a = wl - r;  // float of the row this lane stores in the row's first line
+            float* gr = P.out + rf0 + (size_t)t * 3 * P.Z + a;
+            const float* sr = ob + t * C::OROW + r + a;
+            if (nf == 3 * TZ) {  // a whole row: only the first and last lines are partial
+              if (a >= 0) gr[0] = sr[0];
 #pragma unroll
-          for (int k = 0; k < YPT; ++k) {
-            const bool rowok = (y0 + row0 + k) < P.Y - P.g;
+              for (int i = 1; i < NL - 1; ++i) gr[32 * i] = sr[32 * i];
+              if (a + 32 * (NL - 1) < nf) gr[32 * (NL - 1)] = sr[32 * (NL - 1)];
+            } else {
 #pragma unroll
-            for (int i = 0; i < 3; ++i) {
-              const int f = wl + 32 * i;
-              if (rowok && zspan + f / 3 < P.Z - P.g) ob[k * orow + f] = wb[k * 96 + f];
+              for (int i = 0; i < NL; ++i)
+                if (a + 32 * i >= 0 && a + 32 * i < nf) gr[32 * i] = sr[32 * i];
             }
           }
-          __syncwarp();
+          if (C::OBUFS == 1) asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
         } else if (all_rows) {
 #pragma unroll
           for (int k = 0; k < YPT; ++k) op[k * orow] = res[k][0];
