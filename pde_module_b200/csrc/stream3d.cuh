@@ -277,6 +277,15 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
 #pragma unroll
         for (int m = 0; m < M; ++m) col[m] = sc[rowoff(m) + off[m & 3] + yc];
         float res[YPT][(OP == OP_GRAD) ? 3 : 1];
+        // grad: this plane's staging buffer; tile row t of the plane starts rf0 + 3 Z t
+        // floats into the array, at float (r0 + dzr t) mod 32 of a 128-byte line
+        [[maybe_unused]] float* ob = obuf + (C::OBUFS == 2 ? (opc & 1) * (TY * C::OROW) : 0);
+        [[maybe_unused]] size_t rf0 = 0;
+        [[maybe_unused]] int r0 = 0;
+        if constexpr (OP == OP_GRAD) {
+          rf0 = (((size_t)(xs + j) * P.Y + y0) * P.Z + z0) * 3;
+          r0 = (obase + (int)(rf0 & 31u)) & 31;
+        }
 #pragma unroll
         for (int k = 0; k < YPT; ++k) {
           const float* rowp = sc + rowoff(R + k) + off[(R + k) & 3] + zcmp;
@@ -343,6 +352,13 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
               res[k][2] = az;
             }
           }
+          if constexpr (OP == OP_GRAD) {  // staged at once: the row's results need no registers after this
+            const int t = row0 + k;
+            float* sr = ob + t * C::OROW + ((r0 + t * dzr) & 31) + 3 * lane;
+            sr[0] = res[k][0];
+            sr[1] = res[k][1];
+            sr[2] = res[k][2];
+          }
         }
         release(cs);  // the centre plane is not read again
         adv(cs);
@@ -356,20 +372,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
           // buffers: a buffer is rewritten two planes later, after every consumer
           // has passed the next plane's barrier, i.e. finished reading it; one
           // buffer: a second barrier after the stores.
-          float* ob = obuf + (C::OBUFS == 2 ? (opc & 1) * (TY * C::OROW) : 0);
           ++opc;
-          // tile row t of this plane starts rf0 + 3 Z t floats into the array, at
-          // float (r0 + dzr t) mod 32 of a 128-byte line
-          const size_t rf0 = (((size_t)(xs + j) * P.Y + y0) * P.Z + z0) * 3;
-          const int r0 = (obase + (int)(rf0 & 31u)) & 31;
-#pragma unroll
-          for (int k = 0; k < YPT; ++k) {
-            const int t = row0 + k;
-            float* sr = ob + t * C::OROW + ((r0 + t * dzr) & 31) + 3 * lane;
-            sr[0] = res[k][0];
-            sr[1] = res[k][1];
-            sr[2] = res[k][2];
-          }
           asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
           const int wl = tid & 31;
           const int nf = 3 * min(TZ, P.Z - P.g - z0);  // floats of the row's interior cells
