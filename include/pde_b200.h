@@ -218,10 +218,24 @@ int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* gri
  * ping-pong buffer when nsteps > steps_per_pass).  u_out may equal u_in.
  * steps_per_pass: temporal-blocking depth k (0 = choose).  2D (Z == 1) grids use
  * shared-memory tiles with k steps per pass; 3D grids use k = 1.
- * t0_device: device pointer to the time of the first step (ramp BCs), may be NULL. */
+ * Constant-valued groups only: rules with a ramp group (has_ramp) give
+ * PDE_ERR_UNSUPPORTED here; pde_heat_rollout_at takes them. */
 int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
                      int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
                      int32_t nsteps, int32_t steps_per_pass, void* stream);
+
+/* pde_heat_rollout with time-dependent boundary groups (ramps,
+ * boundary_functions.py:77-92, set through functional_boundary.py:237,254-255,
+ * where the loop passes t to every call).  Step n (0-based) fills the boundary
+ * at t = fp32(t0 + n * t_step), the sum and product taken in double and each
+ * rounded on its own, as a Python loop calling BC(u, t0 + n*dt) computes it;
+ * the result is bit-identical to that loop of the three operators.  t_step is
+ * the time step as a double (the caller's dt before its rounding to fp32).
+ * Constant groups behave as in pde_heat_rollout. */
+int pde_heat_rollout_at(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                        int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
+                        int32_t nsteps, int32_t steps_per_pass, double t0, double t_step,
+                        void* stream);
 
 /* ---- differentiable heat rollout (new: the reference has the forward loop
  * only, examples/2D_Heat_Equation.py:57-65, with a scalar alpha) ----

@@ -249,18 +249,21 @@ def periodic_fill(u: np.ndarray, ghost: int, axes) -> np.ndarray:
 
 # ------------------------------------------------------------- rollouts ---
 def heat_step(u: np.ndarray, groups: list, dx: float, ghost: int, alpha: float, dt: float, order: int = 2,
-              dtype=np.float32) -> np.ndarray:
-    """One step of examples/2D_Heat_Equation.py:59-62 with a zero-ghost Laplacian output."""
-    u2 = bc_apply(u, groups, dx, ghost, dtype=dtype)
+              dtype=np.float32, t: float = 0.0) -> np.ndarray:
+    """One step of examples/2D_Heat_Equation.py:59-62 with a zero-ghost Laplacian
+    output; the boundary is filled at time t (ramp groups)."""
+    u2 = bc_apply(u, groups, dx, ghost, t, dtype=dtype)
     lap = laplacian(u2, dx, ghost, alpha, order, dtype)
     return forward_euler(u2, lap, dt, dtype)
 
 
 def heat_rollout(u: np.ndarray, groups: list, dx: float, ghost: int, alpha: float, dt: float, nsteps: int,
-                 order: int = 2, dtype=np.float32) -> np.ndarray:
+                 order: int = 2, dtype=np.float32, t0: float = 0.0) -> np.ndarray:
+    """nsteps of heat_step; step n fills the boundary at t0 + n*dt (Python floats),
+    as a loop passing that time to GridBoundary does (functional_boundary.py:237,254-255)."""
     u = np.asarray(u, dtype=dtype)
-    for _ in range(nsteps):
-        u = heat_step(u, groups, dx, ghost, alpha, dt, order, dtype)
+    for n in range(nsteps):
+        u = heat_step(u, groups, dx, ghost, alpha, dt, order, dtype, t0 + n * dt)
     return u
 
 

@@ -221,22 +221,29 @@ class GridBoundary(ExplicitUniformGridStencil):
     @property
     def fusable(self) -> bool:
         return (self.periodic_axes == 0 and all(fg.face_mask for fg in self.func_groups.values())
-                and not any(fg.func.kind == "ramp" for fg in self.func_groups.values())
                 and self.inputs[0] <= _lib.PDE_FUSED_MAX_COMP and len(self.func_groups) <= _lib.PDE_MAX_GROUPS)
 
+    @property
+    def time_dependent(self) -> bool:
+        """Some group's value depends on t (a ramp)."""
+        return any(fg.func.kind == "ramp" for fg in self.func_groups.values())
+
     def rules(self) -> "_lib.PdeBCRules":
-        """The groups compiled for the fused kernels (standard face groups only)."""
+        """The groups compiled for the fused kernels (standard face groups only).
+        Ramp groups compile with has_ramp set: the fused heat rollout evaluates them
+        per step (HeatRollout's t0); the other fused solvers reject them."""
         if self._rules is None:
             if not self.fusable:
-                raise NotImplementedError("fused kernels take standard face groups with constant values")
+                raise NotImplementedError("fused kernels take standard face groups")
             n = len(self.func_groups)
             arr = (_lib.PdeBCGroup * max(n, 1))()
             for i, fg in enumerate(self.func_groups.values()):
+                ramp = fg.func.kind == "ramp"
                 arr[i].type = int(fg.boundary_type)
                 arr[i].comp_mask = fg.comp_mask
-                arr[i].func = _lib.PDE_BC_FUNC_CONSTANT
+                arr[i].func = _lib.PDE_BC_FUNC_RAMP if ramp else _lib.PDE_BC_FUNC_CONSTANT
                 arr[i].value = float(fg.func.value)
-                arr[i].t_max = 1.0
+                arr[i].t_max = float(fg.func.t_max) if ramp else 1.0
                 arr[i].face_mask = int(fg.face_mask)
             grid = _lib.make_grid(self.grid_shape, self.ghost_cells, 2, self.dx_value)
             r = _lib.PdeBCRules()

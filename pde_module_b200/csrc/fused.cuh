@@ -139,7 +139,17 @@ struct H2Params {
   int RXM, RYM;    // smem region capacity (cells)
   float w[5];
   float alpha, dt;
+  // time-dependent groups: step n of the rollout fills the boundary at
+  // fp32(t0 + n * tstep), n = n0 + the step within this pass
+  double t0, tstep;
+  int n0;
 };
+
+// Boundary time of rollout step n: t0 + n * tstep in double, each operation
+// rounded on its own (as a host caller computes t0 + n*dt), then rounded to fp32.
+__device__ __forceinline__ float step_time(double t0, double tstep, int n) {
+  return __double2float_rn(__dadd_rn(t0, __dmul_rn((double)n, tstep)));
+}
 
 // Boundary fill of the smem region (array rectangle [rx0,rx0+RX) x [ry0,ry0+RY)),
 // in place: ghosts first (they read pre-boundary interior values), then nodes.
@@ -219,10 +229,14 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
 // region's cut edges move inward R cells per step; the extra cell covers the
 // output ghost cells, whose last boundary fill reads the cell two steps
 // inward (adj) at the previous step.
-template <int R, int N>
+// RAMP: some groups take time-dependent values; the block keeps the rules in
+// shared memory and sets those groups' values for each step before its fill.
+template <int R, int N, bool RAMP>
 __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                         const H2Params P, const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];
+  __shared__ PdeBCRules SR;  // RAMP only: the rules with the current step's group values
+  if (RAMP && threadIdx.x == 0) SR = Rl;
   const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
   const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
   const int H = P.k * R + 1;
@@ -243,7 +257,18 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
   const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(P.X - g, rx0 + RX - R) - rx0;
   const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(P.Y - g, ry0 + RY - R) - ry0;
   for (int s = 0; s < P.k; ++s) {
-    bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    if constexpr (RAMP) {
+      // every read of SR's values in the previous step came before its last barrier
+      const int gi = (int)threadIdx.x;
+      if (gi < Rl.ngroups && Rl.group[gi].func == PDE_BC_FUNC_RAMP) {
+        const float t = step_time(P.t0, P.tstep, P.n0 + s);
+        SR.group[gi].value = bc_value(PDE_BC_FUNC_RAMP, Rl.group[gi].value, Rl.group[gi].t_max, &t);
+      }
+      __syncthreads();
+      bc_fill_region<N>(A, P, SR, rx0, RX, ry0, RY, Rl.dx32);
+    } else {
+      bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    }
     for (int lx = lx0; lx < RX; lx += nrows)
       for (int lf = lf0; lf < nrow; lf += 32) {
         const int idx = lx * nrow + lf;

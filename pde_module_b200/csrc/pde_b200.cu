@@ -475,12 +475,26 @@ int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* gri
   return PDE_OK;
 }
 
-int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
+namespace {
+
+// Host copy of generic.cuh bc_value for a ramp group at rollout step n: the
+// same float operations (t / t_max rounded, min with 1, times the value).
+float host_ramp_value(const PdeBCGroupParam& B, double t0, double tstep, long long n) {
+  const double td = (double)n * tstep;
+  const float t = (float)(t0 + td);
+  const float q = t / B.t_max;
+  const float r = q < 1.0f ? q : 1.0f;
+  return r * B.value;
+}
+
+// The fused rollout; time-dependent groups only when `allow_ramp`.
+int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
                      const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
-                     void* stream) {
+                     bool allow_ramp, double t0, double tstep, void* stream) {
   if (!u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
   if (ncomp < 1 || ncomp > PDE_FUSED_MAX_COMP || rules->ncomp != ncomp) return PDE_ERR_ARG;
-  if (rules->has_ramp) return PDE_ERR_UNSUPPORTED;
+  if (rules->has_ramp && !allow_ramp) return PDE_ERR_UNSUPPORTED;
+  if (rules->ngroups < 0 || rules->ngroups > PDE_MAX_GROUPS) return PDE_ERR_ARG;
   if (work == u_in || work == u_out) return PDE_ERR_ARG;
   Geo G;
   if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
@@ -522,11 +536,12 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
       const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
       for (int t = 0; t < 5; ++t) P.w[t] = W.w[t];
       P.alpha = alpha; P.dt = dt;
+      P.t0 = t0; P.tstep = tstep; P.n0 = done;
       const size_t smem = (size_t)2 * P.RXM * P.RYM * ncomp * sizeof(float);
-      if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+      if (smem > 227 * 1024 - sizeof(PdeBCRules)) return PDE_ERR_TOO_LARGE;
 #define PDE_H2(RR, NN)                                                                                  \
   do {                                                                                                  \
-    auto kern = heat2d_tb_kernel<RR, NN>;                                                               \
+    auto kern = rules->has_ramp ? heat2d_tb_kernel<RR, NN, true> : heat2d_tb_kernel<RR, NN, false>;      \
     PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);                                                \
   } while (0)
@@ -548,8 +563,13 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
 #undef PDE_H2
     } else {
       const int64_t total = G.n[0] * G.n[1] * G.n[2] * ncomp;
-      if (R == 1) heat_step_kernel<1><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, *rules, total);
-      else heat_step_kernel<2><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, *rules, total);
+      // one step per launch: time-dependent group values are set in a copy of the rules
+      PdeBCRules Rs = *rules;
+      if (rules->has_ramp)
+        for (int i = 0; i < rules->ngroups; ++i)
+          if (rules->group[i].func == PDE_BC_FUNC_RAMP) Rs.group[i].value = host_ramp_value(rules->group[i], t0, tstep, done);
+      if (R == 1) heat_step_kernel<1><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, Rs, total);
+      else heat_step_kernel<2><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, Rs, total);
     }
     int rc = launch_status();
     if (rc) return rc;
@@ -559,6 +579,22 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
   }
   if (need_copy) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, work, bytes, cudaMemcpyDeviceToDevice, st));
   return PDE_OK;
+}
+
+}  // namespace
+
+int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
+                     const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
+                     void* stream) {
+  return heat_rollout_run(u_in, u_out, work, grid, ncomp, rules, alpha, dt, nsteps, steps_per_pass, false, 0.0, 0.0,
+                          stream);
+}
+
+int pde_heat_rollout_at(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
+                        const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
+                        double t0, double t_step, void* stream) {
+  return heat_rollout_run(u_in, u_out, work, grid, ncomp, rules, alpha, dt, nsteps, steps_per_pass, true, t0, t_step,
+                          stream);
 }
 
 namespace {

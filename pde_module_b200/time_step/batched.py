@@ -153,6 +153,8 @@ class BatchedHeatRollout(_BatchedRollout):
             boundary.dirichlet_BC("ALL", 0.0)
         if boundary.inputs[0] != 1:
             raise ValueError("batched heat rollouts take scalar fields")
+        if boundary.time_dependent:
+            raise NotImplementedError("batched heat rollouts take constant-valued boundary groups")
         self.boundary = boundary
         self._setup(fields, None, dx, alpha, dt, boundary.rules(), ghost_cells, order, tile, steps_per_pass)
 

@@ -36,17 +36,23 @@ class HeatRollout:
         self.output_array = None
         self.work = None
 
-    def __call__(self, u: torch.Tensor, nsteps: int) -> torch.Tensor:
+    def __call__(self, u: torch.Tensor, nsteps: int, t0: float = 0.0) -> torch.Tensor:
+        """Advance ``nsteps``; step n fills the boundary at time t0 + n*dt (only
+        ramp groups depend on it), as the loop ``u2 = bc(u, t0 + n*dt)`` does."""
         require_cuda_f32(u, "u")
         if tuple(u.shape) != tuple(self.boundary.grid_shape) + (self.ncomp,):
             raise AssertionError(f"field shape {tuple(u.shape)} does not match the boundary's grid")
         if self.output_array is None:
             self.output_array = torch.zeros_like(u)
             self.work = torch.zeros_like(u)
-        check(lib().pde_heat_rollout(C.c_void_p(u.data_ptr()), C.c_void_p(self.output_array.data_ptr()),
-                                     C.c_void_p(self.work.data_ptr()), C.byref(self.grid), self.ncomp,
-                                     C.byref(self.rules), self.alpha, self.dt, int(nsteps), self.steps_per_pass,
-                                     C.c_void_p(stream_ptr(u))), "pde_heat_rollout")
+        args = [C.c_void_p(u.data_ptr()), C.c_void_p(self.output_array.data_ptr()), C.c_void_p(self.work.data_ptr()),
+                C.byref(self.grid), self.ncomp, C.byref(self.rules), self.alpha, self.dt, int(nsteps),
+                self.steps_per_pass]
+        if self.rules.has_ramp:
+            check(lib().pde_heat_rollout_at(*args, float(t0), self.dt, C.c_void_p(stream_ptr(u))),
+                  "pde_heat_rollout_at")
+        else:
+            check(lib().pde_heat_rollout(*args, C.c_void_p(stream_ptr(u))), "pde_heat_rollout")
         return self.output_array
 
 
@@ -75,6 +81,8 @@ class HeatSolver:
         self.shape = tuple(boundary.grid_shape)
         assert self.shape[2] == 1 and self.shape[0] > 1 and self.shape[1] > 1, "2D grids (X, Y, 1)"
         self.dx, self.dt, self.N, self.order = float(dx), float(dt), int(nsteps), int(order)
+        if boundary.time_dependent:
+            raise NotImplementedError("HeatSolver takes constant-valued boundary groups")
         self.rules = boundary.rules()
         self.grid = make_grid(self.shape, boundary.ghost_cells, self.order, self.dx)
         self._steps_per_pass = int(steps_per_pass)

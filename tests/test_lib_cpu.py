@@ -45,6 +45,27 @@ def test_argument_validation_needs_no_gpu():
     assert L.pde_bc_compile(grp, 1, C.byref(g), 1, C.byref(r)) == _lib.PDE_ERR_UNSUPPORTED
 
 
+def test_ramp_rules_compile_and_only_the_timed_rollout_takes_them():
+    """A ramp group compiles with has_ramp set; pde_heat_rollout (constant groups)
+    refuses such rules before touching any memory, pde_heat_rollout_at validates
+    its arguments the same way."""
+    L = _lib.lib()
+    g = _lib.make_grid((8, 8, 1), 1, 2, 0.1)
+    grp = (_lib.PdeBCGroup * 2)()
+    grp[0].type, grp[0].comp_mask, grp[0].face_mask, grp[0].func, grp[0].value = 1, 1, 0xF, 0, 0.0
+    grp[1].type, grp[1].comp_mask, grp[1].face_mask = 1, 1, 1 << 3  # +Y
+    grp[1].func, grp[1].value, grp[1].t_max = _lib.PDE_BC_FUNC_RAMP, 1.0, 0.5
+    r = _lib.PdeBCRules()
+    assert L.pde_bc_compile(grp, 2, C.byref(g), 1, C.byref(r)) == _lib.PDE_OK
+    assert r.has_ramp == 1 and r.group[1].func == _lib.PDE_BC_FUNC_RAMP and r.group[1].t_max == 0.5
+    p = [C.c_void_p(16), C.c_void_p(32), C.c_void_p(48)]
+    assert L.pde_heat_rollout(*p, C.byref(g), 1, C.byref(r), 1.0, 1e-3, 4, 0, None) == _lib.PDE_ERR_UNSUPPORTED
+    assert L.pde_heat_rollout_at(None, None, None, C.byref(g), 1, C.byref(r), 1.0, 1e-3, 4, 0, 0.0, 1e-3,
+                                 None) == _lib.PDE_ERR_ARG
+    assert L.pde_heat_rollout_at(*p, C.byref(g), 2, C.byref(r), 1.0, 1e-3, 4, 0, 0.0, 1e-3,
+                                 None) == _lib.PDE_ERR_ARG  # ncomp differs from the rules'
+
+
 # ---- rule compiler ----------------------------------------------------------
 def compile_rules(shape, g, ncomp, spec, dx=0.1):
     """spec: (name, type, value, comps)"""
