@@ -400,6 +400,41 @@ int pde_batch_plan(int32_t kind, const PdeBatchGrid* grids, int32_t ngrids, int3
  * kernel launch, so it can be captured in a CUDA graph. */
 int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream);
 
+/* ---- immersed boundary (FDM/boundary/immersedBoundary.py) ----
+ * Solid regions inside the grid given by an int8 bitmask (X, Y, Z), nonzero =
+ * solid, with the reference's staircase boundary.  Solid cells must not lie on
+ * the array's outer layer along an eligible axis (the reference reads outside
+ * the array there): such bitmasks give PDE_ERR_ARG. */
+
+/* Scratch bytes pde_ib_maps needs for a grid (-1 for an invalid grid). */
+int64_t pde_ib_work_bytes(const PdeGrid* grid);
+
+/* The index maps of finalize() (immersedBoundary.py:57-151, kernels :344-438),
+ * each list in C order as the reference's np.nonzero / np.unique give them:
+ *   solid_boundary  (n_sb x 3 int32): solid cells with a fluid neighbour along an eligible axis
+ *   fluid_neighbors (n_sb x D x 2 int8): the bitmask at -1 / +1 along each eligible axis
+ *   interior_solids (n_is x 3 int32): the other solid cells
+ *   fluid_boundary  (n_fb x 3 int32): fluid cells next to a solid cell
+ * counts[3] receives (n_sb, n_is, n_fb).  With solid_boundary NULL only the counts
+ * are computed (size the lists, then call again).  Synchronises the stream (the
+ * counts come back to the host); not for stream capture.  work: pde_ib_work_bytes. */
+int pde_ib_maps(const int8_t* bitmask, const PdeGrid* grid, int32_t* solid_boundary,
+                int8_t* fluid_neighbors, int32_t* interior_solids, int32_t* fluid_boundary,
+                int64_t* counts, void* work, int64_t work_bytes, void* stream);
+
+/* forward(u, fill_value) of the immersed boundary (immersedBoundary.py:176-298):
+ * out = in (copied unless out == in), then for each boundary cell and component
+ * (bc_type / bc_value: n_boundary x ncomp, row-major) PDE_BC_DIRICHLET sets the
+ * value and PDE_BC_VON_NEUMANN the running mean over the fluid neighbours of
+ * (u_f - (s * value) * dx), s = -1 / +1, every operation rounded on its own (other
+ * types leave the cell as it is); then every interior solid cell takes fill_value
+ * in all components.  out may equal in.  Bit-identical to the reference. */
+int pde_ib_apply(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
+                 const int32_t* solid_boundary, const int8_t* fluid_neighbors,
+                 const int8_t* bc_type, const float* bc_value, int64_t n_boundary,
+                 const int32_t* interior_solids, int64_t n_interior, float fill_value,
+                 void* stream);
+
 /* Allocation-free variant of pde_heat_rollout.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a memory manager
  * owns every allocation, cudaMalloc is not allowed in a latency-critical loop,

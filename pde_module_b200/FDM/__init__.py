@@ -1,4 +1,4 @@
 """Finite-difference operators on uniform grids (reference: FDM/__init__.py)."""
 from .module import Laplacian, Grad, Divergence, ExplicitUniformGridStencil
-from .boundary import GridBoundary
+from .boundary import GridBoundary, ImmersedBoundary
 from . import kernel, functional, module, boundary

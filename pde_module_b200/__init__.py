@@ -5,13 +5,13 @@ their functional forms) over torch CUDA float32 tensors, backed by the C ABI
 of include/pde_b200.h in ``_native/libpde_b200.so``.
 """
 from . import _lib
-from .FDM import Laplacian, Grad, Divergence, GridBoundary
+from .FDM import Laplacian, Grad, Divergence, GridBoundary, ImmersedBoundary
 from .time_step import (ForwardEuler, HeatRollout, HeatSolver, heat_rollout, FractionalStepLDC,
                         SlabFractionalStepLDC, WaveSolver,
                         wave_rollout,
                         BatchedHeatRollout, BatchedWaveRollout)
 from .mesh import UniformGridMesh, create_structured_field, create_structured_warp_field
 
-__all__ = ["Laplacian", "Grad", "Divergence", "GridBoundary", "ForwardEuler", "HeatRollout", "FractionalStepLDC", "SlabFractionalStepLDC",
+__all__ = ["Laplacian", "Grad", "Divergence", "GridBoundary", "ImmersedBoundary", "ForwardEuler", "HeatRollout", "FractionalStepLDC", "SlabFractionalStepLDC",
            "HeatSolver", "heat_rollout", "WaveSolver", "wave_rollout", "BatchedHeatRollout", "BatchedWaveRollout",
            "UniformGridMesh", "create_structured_field", "create_structured_warp_field"]

@@ -127,6 +127,11 @@ _SIGS = {
     "pde_heat_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                    C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                    C.c_void_p]),
+    "pde_ib_work_bytes": (C.c_int64, [C.POINTER(PdeGrid)]),
+    "pde_ib_maps": (C.c_int, [C.c_void_p, C.POINTER(PdeGrid), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.POINTER(C.c_int64), C.c_void_p, C.c_int64, C.c_void_p]),
+    "pde_ib_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_float, C.c_void_p]),
     "pde_heat_rollout_at": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                       C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                       C.c_double, C.c_double, C.c_void_p]),

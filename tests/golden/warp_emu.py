@@ -20,7 +20,9 @@ Semantics reproduced (Warp's documented kernel semantics):
     path have no write-after-read hazards between threads, so sequential order
     gives the result of any parallel order;
   * ``wp.empty`` fills float storage with NaN so cells a kernel never writes
-    are visible as such.
+    are visible as such;
+  * NumPy arrays passed to a launch are wrapped without a copy (Warp's CPU
+    behaviour), and ``arr[i]`` of a 2-d array is a view of row i.
 Kernel bodies are compiled from their source (``inspect.getsource``) with the
 closure variables of the reference's kernel factories bound at first launch,
 the same information Warp's own code generator resolves.
@@ -306,6 +308,14 @@ class _Array:
         return idx
 
     def __getitem__(self, idx):
+        if not isinstance(idx, tuple):
+            idx = (idx,)
+        if len(idx) < len(self.shape):  # arr[i] of a 2-d array: a view of row i
+            sub = tuple(int(i) for i in idx)
+            for i, n in zip(sub, self.shape):
+                if i < 0 or i >= n:
+                    raise IndexError(f"index {sub} out of bounds for shape {self.shape}")
+            return _Array(self.st[sub], self.dtype, self.shape[len(sub):])
         idx = self._idx(idx)
         if type_is_vector(self.dtype) or type_is_matrix(self.dtype):
             return self.dtype._wrap(self.st[idx].copy())
@@ -324,7 +334,7 @@ class _Array:
         return self.st
 
     def fill_(self, v):
-        self.st[...] = v
+        self.st[...] = v.d if isinstance(v, (_Vec, _Mat)) else v
 
     def zero_(self):
         self.st[...] = 0
@@ -334,7 +344,10 @@ def _make_array(data=None, dtype=None, shape=None, device=None, copy=True, **kw)
     if data is None and shape is None:
         return _Ann("array", dtype)
     if dtype is None:
-        dtype = np.float32
+        # Warp takes the element type of a NumPy array; the path's integer and
+        # boolean arrays (ImmersedBoundary's type table) keep theirs, others are float32
+        src_dt = getattr(data, "dtype", None)
+        dtype = src_dt.type if src_dt is not None and src_dt.type in (np.int8, np.int32, np.bool_) else np.float32
     es = _elem_shape(dtype)
     npdt = _storage_np(dtype)
     if data is None:
@@ -495,6 +508,15 @@ def kernel(fn=None, **kw):
 
 
 def _convert(arg, ann):
+    if isinstance(arg, np.ndarray) and isinstance(ann, _Ann):
+        # a NumPy array passed to a CPU launch: Warp wraps its memory without a
+        # copy, so the kernel's stores land in the caller's array
+        dt = ann.dtype if ann.dtype is not None else arg.dtype.type
+        if dt is bool:
+            dt = np.bool_
+        es = _elem_shape(dt)
+        assert arg.dtype == np.dtype(_storage_np(dt)), f"{arg.dtype} array for a {dt} parameter"
+        return _Array(arg, dt, arg.shape[:arg.ndim - len(es)] if es else arg.shape)
     if isinstance(ann, type) and ann in (np.float32, np.float64, np.int32, np.int8, np.uint8):
         return ann(arg)
     if ann is float:
