@@ -435,6 +435,30 @@ int pde_ib_apply(const float* in, float* out, const PdeGrid* grid, int32_t ncomp
                  const int32_t* interior_solids, int64_t n_interior, float fill_value,
                  void* stream);
 
+/* ---- element-wise and absorbing-layer operators (weakly compressible / ACM path) ---- */
+
+/* OuterProduct (FDM/module/elementWiseOps.py:10-48): per cell c,
+ * out[c][i][j] = a[c][i] * b[c][j]; a: cells x na, b: cells x nb, out: cells x na x nb. */
+int pde_outer(const float* a, const float* b, float* out, int64_t cells, int32_t na, int32_t nb,
+              void* stream);
+
+/* scalarVectorMult (elementWiseOps.py:51-88, FDM/kernel/elementWiseOps.py:6-23):
+ * out[c][k] = s[c] * b[c][k]; s: one float per cell, b and out: cells x nb. */
+int pde_scalar_mult(const float* s, const float* b, float* out, int64_t cells, int32_t nb, void* stream);
+
+/* FarField / ViscousDampingLayer on their layer points (FDM/kernel/farfield.py:50-77,
+ * FDM/kernel/viscousDampingLayer.py:50-76).  For point p (flat cell index cells[p],
+ * ncomp floats per cell) and component k, with damp = scale * profile[p]:
+ *   cond_host != NULL (FarField):    out = -damp * (in - cond_host[k])
+ *   cond_host == NULL (damping):     out = -damp * in
+ * each operation rounded on its own; other cells of out are not written.
+ * profile[p] = (dx / L) ** exponent, the layer depth of the point over its
+ * thickness, prepared by the caller (once per layer).  cond_host: up to 16 host
+ * floats (the far-field vector or matrix), copied into the launch. */
+int pde_layer_apply(const float* in, float* out, int32_t ncomp, const int64_t* cells,
+                    const float* profile, int64_t npoints, float scale, const float* cond_host,
+                    void* stream);
+
 /* Allocation-free variant of pde_heat_rollout.  No counterpart in the
  * reference.  For callers that cannot allocate device memory (a memory manager
  * owns every allocation, cudaMalloc is not allowed in a latency-critical loop,

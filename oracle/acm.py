@@ -1,0 +1,124 @@
+"""ORACLE — TEST INFRASTRUCTURE ONLY.
+
+CPU (NumPy) restatement of PDE_Module's element-wise, absorbing-layer and
+Runge-Kutta modules, used by tests/ as the checker.  Nothing in pde_module_b200
+imports it.
+
+* OuterProduct — FDM/module/elementWiseOps.py:10-48 (wp.outer per cell: M[i, j] =
+  A[i] * B[j], one rounding per product).
+* scalarVectorMult — elementWiseOps.py:51-88, FDM/kernel/elementWiseOps.py:6-23
+  (a[0] * b per cell).
+* FarField — FDM/module/farfield.py:13-151, FDM/kernel/farfield.py:8-77: points of
+  the outer layers (per eligible axis, index < L or >= n - L, excluded groups left
+  out, :62-90); per point the axis of the nearest array face (first minimum,
+  :38-48), the depth dx into the layer (:66-70) and
+  out = -(sigma * (dx / L) ** beta) * (u - u_far); zero elsewhere.
+* ViscousDampingLayer — FDM/module/viscousDampingLayer.py:13-150,
+  FDM/kernel/viscousDampingLayer.py:8-76: the same points and depth,
+  out = -(C_max * (dx / L) ** p) * du_dt.
+* RungeKatta1 / RungeKatta2 — time_step/rungeKatta.py:21-174, composed from the
+  fdm oracle's GridBoundary, Laplacian and ForwardEuler (RungeKatta1 steps with
+  dt / 2, as the reference does, :79-83).
+
+The layer profile (dx / L) ** beta is a float32 power (the C library's powf, as
+the reference's CPU kernels and NumPy's float32 scalar power both call).
+
+Parity pin: tests/golden/make_acm_golden.py runs the reference modules through
+tests/golden/warp_emu.py (tests/golden/acm_golden.npz); tests/test_acm_cpu.py
+checks this restatement against them bit for bit.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import fdm
+
+INT32_MAX = 2 ** 31 - 1
+
+
+def outer(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    return (A[..., :, None] * B[..., None, :]).astype(np.float32)
+
+
+def scalar_mult(A: np.ndarray, B: np.ndarray) -> np.ndarray:
+    s = A[..., 0].astype(np.float32)
+    return (s.reshape(s.shape + (1,) * (B.ndim - 3)) * B).astype(np.float32)
+
+
+def layer_points(grid_shape, num_layers: int, exclude=()) -> np.ndarray:
+    """(n, 3) int32 points of the absorbing layers, in C order (farfield.py:62-90)."""
+    idx = np.moveaxis(np.indices(grid_shape, dtype=np.int32), 0, -1).reshape(-1, 3)
+    masks = []
+    for i, (s, ax) in enumerate(zip(grid_shape, "XYZ")):
+        if s > 1:
+            if f"-{ax}" not in exclude:
+                masks.append(idx[:, i] < num_layers)
+            if f"+{ax}" not in exclude:
+                masks.append(idx[:, i] >= s - num_layers)
+    mask = masks[0]
+    for m in masks[1:]:
+        mask = np.logical_or(mask, m)
+    return idx[mask]
+
+
+def layer_depth(points: np.ndarray, grid_shape, num_layers: int) -> np.ndarray:
+    """Depth dx of each point into its layer (farfield.py:38-48, :62-70)."""
+    n = np.array(grid_shape, dtype=np.int64)
+    p = points.astype(np.int64)
+    dist = np.where(n > 1, np.minimum(p, n - p - 1), INT32_MAX)
+    axis = np.argmin(dist, axis=1)  # first minimum
+    x = p[np.arange(len(p)), axis]
+    na = n[axis]
+    hi_lim = (na - 1) - num_layers
+    return np.where((na - 1 - x) < x, x - hi_lim, num_layers - x)
+
+
+def layer_profile(points, grid_shape, num_layers: int, exponent: float) -> np.ndarray:
+    """(dx / L) ** exponent per point, in float32, one powf each."""
+    d = layer_depth(points, grid_shape, num_layers)
+    q = d.astype(np.float32) / np.float32(num_layers)
+    e = np.float32(exponent)
+    return np.array([np.float32(v) ** e for v in q], dtype=np.float32)
+
+
+def farfield(u: np.ndarray, grid_shape, num_layers: int, beta: float, cond, sigma: float, exclude=()):
+    pts = layer_points(grid_shape, num_layers, exclude)
+    prof = layer_profile(pts, grid_shape, num_layers, beta)
+    out = np.zeros_like(u, dtype=np.float32)
+    damp = (np.float32(sigma) * prof).astype(np.float32)
+    c = np.asarray(cond, dtype=np.float32).reshape(u.shape[3:])
+    sel = (pts[:, 0], pts[:, 1], pts[:, 2])
+    diff = (u[sel] - c).astype(np.float32)
+    out[sel] = ((-damp).reshape((-1,) + (1,) * (u.ndim - 3)) * diff).astype(np.float32)
+    return out
+
+
+def damping(du: np.ndarray, grid_shape, num_layers: int, p: float, cmax: float, exclude=()):
+    pts = layer_points(grid_shape, num_layers, exclude)
+    prof = layer_profile(pts, grid_shape, num_layers, p)
+    out = np.zeros_like(du, dtype=np.float32)
+    damp = (np.float32(cmax) * prof).astype(np.float32)
+    sel = (pts[:, 0], pts[:, 1], pts[:, 2])
+    out[sel] = ((-damp).reshape((-1,) + (1,) * (du.ndim - 3)) * du[sel]).astype(np.float32)
+    return out
+
+
+def runge_kutta(order: int, fields, groups, alphas, dx, ghost, dt, steps):
+    """RungeKatta1/2 with bc = GridBoundary per field and f = Laplacian(alpha) per field.
+    Ghost cells of the Laplacian output are taken as zero (the reference's output
+    there is never written)."""
+    ys = [np.asarray(u, dtype=np.float32) for u in fields]
+    t = 0.0
+    for _ in range(steps):
+        ys = [fdm.bc_apply(y, g, dx, ghost, t) for y, g in zip(ys, groups)]
+        k1 = [fdm.laplacian(y, dx, ghost, a) for y, a in zip(ys, alphas)]
+        if order == 1:
+            ys = [fdm.forward_euler(y, k, dt / 2) for y, k in zip(ys, k1)]
+        else:
+            y0 = [y.copy() for y in ys]
+            y1 = [fdm.forward_euler(y, k, dt / 2) for y, k in zip(ys, k1)]
+            y1 = [fdm.bc_apply(y, g, dx, ghost, t) for y, g in zip(y1, groups)]
+            k2 = [fdm.laplacian(y, dx, ghost, a) for y, a in zip(y1, alphas)]
+            ys = [fdm.forward_euler(y, k, dt) for y, k in zip(y0, k2)]
+        t += dt
+    return ys

@@ -132,6 +132,10 @@ _SIGS = {
                               C.POINTER(C.c_int64), C.c_void_p, C.c_int64, C.c_void_p]),
     "pde_ib_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32, C.c_void_p, C.c_void_p,
                                C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_float, C.c_void_p]),
+    "pde_outer": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_int32, C.c_void_p]),
+    "pde_scalar_mult": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
+    "pde_layer_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_float,
+                                  C.c_void_p, C.c_void_p]),
     "pde_heat_rollout_at": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                       C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                       C.c_double, C.c_double, C.c_void_p]),

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libpde_b200.so")
 
-SOURCES = ["pde_b200.cu", "noalloc.cu", "immersed.cu"]
+SOURCES = ["pde_b200.cu", "noalloc.cu", "immersed.cu", "acm.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",

@@ -22,7 +22,9 @@ Semantics reproduced (Warp's documented kernel semantics):
   * ``wp.empty`` fills float storage with NaN so cells a kernel never writes
     are visible as such;
   * NumPy arrays passed to a launch are wrapped without a copy (Warp's CPU
-    behaviour), and ``arr[i]`` of a 2-d array is a view of row i.
+    behaviour), and ``arr[i]`` of a 2-d array is a view of row i;
+  * kernel ``assert`` statements are not executed (Warp's default "release"
+    mode compiles them out).
 Kernel bodies are compiled from their source (``inspect.getsource``) with the
 closure variables of the reference's kernel factories bound at first launch,
 the same information Warp's own code generator resolves.
@@ -430,6 +432,16 @@ def max(a, b):  # noqa: A001
     return a if a > b else b
 
 
+def outer(a, b):
+    """wp.outer: the matrix a b^T, each product rounded on its own."""
+    return matrix((a._length_, b._length_), a._np)._wrap(np.outer(a.d, b.d).astype(a._np))
+
+
+def argmin(v):
+    """wp.argmin: index of the first smallest component."""
+    return int(np.argmin(v.d))
+
+
 def _setc(arr, idx, comp, value):
     e = arr[idx]
     e[comp] = value
@@ -437,7 +449,11 @@ def _setc(arr, idx, comp, value):
 
 
 class _StoreRewrite(ast.NodeTransformer):
-    """`A[i, j, k][c] = v`  ->  `__wp_setc(A, (i, j, k), c, v)`"""
+    """`A[i, j, k][c] = v`  ->  `__wp_setc(A, (i, j, k), c, v)`; kernel ``assert``
+    statements are dropped, as Warp's default release mode compiles them out."""
+
+    def visit_Assert(self, node):
+        return ast.Pass()
 
     def visit_Assign(self, node):
         self.generic_visit(node)
