@@ -232,8 +232,8 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
 // RAMP: some groups take time-dependent values; the block keeps the rules in
 // shared memory and sets those groups' values for each step before its fill.
 template <int R, int N, bool RAMP>
-__global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict__ in, float* __restrict__ out,
-                                                        const H2Params P, const PdeBCRules Rl) {
+__global__ void __launch_bounds__(1024) heat2d_tb_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                         const H2Params P, const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];
   __shared__ PdeBCRules SR;  // RAMP only: the rules with the current step's group values
   if (RAMP && threadIdx.x == 0) SR = Rl;
@@ -246,10 +246,14 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
   float* A = sm;
   float* B = sm + P.RXM * P.RYM * N;
   const int nrow = RY * N;  // floats per region row
-  // 2D thread layout: 32 lanes along the contiguous (y, component) floats, blockDim.x / 32 rows
-  const int lf0 = threadIdx.x & 31, lx0 = threadIdx.x >> 5, nrows = blockDim.x >> 5;
-  for (int lx = lx0; lx < RX; lx += nrows)
-    for (int lf = lf0; lf < nrow; lf += 32) cp_async4(A + lx * nrow + lf, in + ((size_t)(rx0 + lx) * P.Y + ry0) * N + lf, true);
+  const int nt = (int)blockDim.x, RF = RX * nrow;
+  // flat walk over the region's floats (rows of nrow contiguous floats): consecutive
+  // threads take consecutive floats, every thread has the same share
+  {
+    RectWalk wk(nrow, nt);
+    for (int i = threadIdx.x; i < RF; i += nt, wk.next())
+      cp_async4(A + i, in + ((size_t)(rx0 + wk.row) * P.Y + ry0) * N + wk.col, true);
+  }
   cp_async_wait_all();
   __syncthreads();
   const int g = P.g;
@@ -269,22 +273,21 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
     } else {
       bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
     }
-    for (int lx = lx0; lx < RX; lx += nrows)
-      for (int lf = lf0; lf < nrow; lf += 32) {
-        const int idx = lx * nrow + lf;
-        const int ly = lf / N;
-        const float u2 = A[idx];
-        float res = u2;
-        if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
-          float acc = 0.0f;
+    RectWalk wk(nrow, nt);
+    for (int idx = threadIdx.x; idx < RF; idx += nt, wk.next()) {
+      const int lx = wk.row, ly = wk.col / N;
+      const float u2 = A[idx];
+      float res = u2;
+      if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
+        float acc = 0.0f;
 #pragma unroll
-          for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * nrow]));
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * nrow]));
 #pragma unroll
-          for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * N]));
-          res = add(u2, mul(P.dt, mul(P.alpha, acc)));
-        }
-        B[idx] = res;
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], A[idx + (t - R) * N]));
+        res = add(u2, mul(P.dt, mul(P.alpha, acc)));
       }
+      B[idx] = res;
+    }
     __syncthreads();
     float* tmp = A;
     A = B;
@@ -294,9 +297,9 @@ __global__ void __launch_bounds__(256) heat2d_tb_kernel(const float* __restrict_
   // (non-stencil cells copy their filled value through).
   const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
   const int onrow = (oy1 - by0) * N;
-  for (int lx = lx0; lx < ox1 - bx0; lx += nrows)
-    for (int lf = lf0; lf < onrow; lf += 32)
-      out[((size_t)(bx0 + lx) * P.Y + by0) * N + lf] = A[(bx0 + lx - rx0) * nrow + (by0 - ry0) * N + lf];
+  RectWalk wo(onrow, nt);
+  for (int i = threadIdx.x; i < (ox1 - bx0) * onrow; i += nt, wo.next())
+    out[((size_t)(bx0 + wo.row) * P.Y + by0) * N + wo.col] = A[(bx0 + wo.row - rx0) * nrow + (by0 - ry0) * N + wo.col];
 }
 
 }  // namespace pde

@@ -2,6 +2,7 @@
 // One translation unit: every kernel header is included here so the library
 // has a single device-side error word.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <string.h>
 
 #include "common.cuh"
@@ -31,6 +32,11 @@ int sm_count() {
 }
 
 int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ERR_CUDA; }
+
+// Launch shape of the temporally blocked 2D kernels set by pde_set_launch_2d
+// (tile sides, threads per block); 0 = each entry point's own choice.
+int g_tile2d[2] = {0, 0};
+int g_threads2d = 0;
 
 // A 2D tile count just above m x SMs (m = 1, 2) leaves a short tail wave in which
 // a few SMs run a second tile while the rest wait: enlarge the tiles slightly
@@ -529,8 +535,24 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
     if (two_d) {
       H2Params P;
       P.X = (int)G.n[0]; P.Y = (int)G.n[1]; P.g = G.g; P.N = ncomp; P.k = ks;
-      P.TBX = 16; P.TBY = 32;
       const int H = k * R + 1;  // must match heat2d_tb_kernel
+      // Automatic shape: square tiles of about one per SM (sides 16..64, balanced
+      // against the SM count), 512 threads; 16x32 tiles when those regions would
+      // not fit in shared memory.
+      int threads = g_threads2d > 0 ? g_threads2d : 512;
+      if (g_tile2d[0] > 0) {  // pde_set_launch_2d
+        P.TBX = g_tile2d[0];
+        P.TBY = g_tile2d[1];
+      } else {
+        int t = (int)ceil(sqrt((double)P.X * P.Y / sm_count()));
+        t = t < 16 ? 16 : (t > 64 ? 64 : t);
+        P.TBX = P.TBY = t;
+        balance_tiles(P.X, P.Y, &P.TBX, &P.TBY);
+        if ((size_t)2 * (P.TBX + 2 * H) * (P.TBY + 2 * H) * ncomp * sizeof(float) > 227 * 1024 - sizeof(PdeBCRules)) {
+          P.TBX = 16;
+          P.TBY = 32;
+        }
+      }
       P.RXM = P.TBX + 2 * H; P.RYM = P.TBY + 2 * H;
       P.tiles_y = (P.Y + P.TBY - 1) / P.TBY;
       const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
@@ -543,7 +565,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
   do {                                                                                                  \
     auto kern = rules->has_ramp ? heat2d_tb_kernel<RR, NN, true> : heat2d_tb_kernel<RR, NN, false>;      \
     PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-    kern<<<tiles, 256, smem, st>>>(src, dst, P, *rules);                                                \
+    kern<<<tiles, threads, smem, st>>>(src, dst, P, *rules);                                            \
   } while (0)
       if (R == 1) {
         switch (ncomp) {
@@ -602,8 +624,6 @@ namespace {
 // Output tile of the temporally blocked 2D kernels (differentiable heat, wave,
 // cavity): the largest of 32x64, 32x32, 16x32 that still gives every SM a tile,
 // balanced against the SM count, unless pde_set_launch_2d fixed one.
-int g_tile2d[2] = {0, 0};
-int g_threads2d = 0;
 
 // Threads per block for the wave kernels: enough warps per SM to hide shared-
 // memory latency when tiles are few (up to 1024), 256 when every SM has several.

@@ -1,8 +1,8 @@
 """Launch shapes of the temporally blocked 2D kernels leave results unchanged: odd
 tile sides set with pde_set_launch_2d, and the automatic tiles that are balanced
 against the SM count on grids with a little more than one tile per SM, give the
-oracle's values bit for bit (differentiable heat, wave, cavity; the fused heat
-rollout at a size with more tiles than SMs)."""
+oracle's values bit for bit (fused heat rollout, differentiable heat, wave,
+cavity)."""
 import numpy as np
 import pytest
 import torch
@@ -139,9 +139,28 @@ def test_cavity_odd_tiles(tile, launch):
     assert np.array_equal(s.p.cpu().numpy(), p)
 
 
+@pytest.mark.parametrize("tile", ODD + [(16, 32, 256)])
+def test_fused_heat_rollout_odd_tiles(tile, launch):
+    """The fused rollout under pde_set_launch_2d shapes, several components and a
+    mixed boundary, 13 steps in passes of 5, against the oracle."""
+    shape, g, N = (47, 53, 1), 1, 2
+    dx = 1.0 / 44
+    dt = 0.2 * dx * dx
+    spec = [("ALL", 1, 0.0, (0, 1)), ("+Y", 2, 0.5, (1,)), ("-X", 1, 1.0, (0,))]
+    u0 = np.random.default_rng(17).random(shape + (N,)).astype(np.float32)
+    ud = torch.from_numpy(u0).cuda()
+    bc = P.GridBoundary(ud, dx, g)
+    for nm, typ, val, comps in spec:
+        bc.set_BC(nm, val, typ, comps)
+    launch(*tile)
+    out = P.HeatRollout(bc, dx, 0.8, dt, steps_per_pass=5)(ud, 13)
+    ref = fdm.heat_rollout(u0, fdm.standard_groups(shape, g, spec), dx, g, 0.8, dt, 13)
+    assert np.array_equal(out.cpu().numpy(), ref)
+
+
 def test_fused_heat_rollout_at_258():
-    """153 tiles of 16x32 on a 258^2 array, 256 threads each (several blocks per
-    SM); 20 steps agree with the oracle bit for bit."""
+    """The automatic shape on a 258^2 array (22x22 tiles, one per SM, 512 threads);
+    20 steps agree with the oracle bit for bit."""
     shape, g = (258, 258, 1), 1
     dx = 1.0 / 256
     dt = 0.2 * dx * dx
