@@ -948,7 +948,7 @@ def run_profile_op(args):
     --iters timed calls.  --profile-op is lap2|lap4|grad2|grad4|div2|div4."""
     import torch
     import pde_module_b200 as P
-    if args.profile_op in ("wave", "heatadj", "batched", "ldc"):
+    if args.profile_op in ("wave", "heatadj", "batched", "ldc", "heat"):
         return run_profile_2d(args)
     op, order = args.profile_op[:-1], int(args.profile_op[-1])
     n = args.profile_n
@@ -983,6 +983,7 @@ def run_profile_op(args):
 def run_profile_2d(args):
     """The 2D time-stepping kernels for profilers, eager (no graphs), short runs:
     wave    - 512^2 wave problem, 96 steps, forward + adjoint (k = 4, automatic tile)
+    heat    - 256^2 fused heat rollout (Dirichlet 0), 96 steps (k = 8, automatic launch shape)
     heatadj - 256^2 heat, alpha field, 96 steps, forward + adjoint (k = 4)
     batched - the 64-grid batched heat rollout, 16 steps (k = 4, 64 x 64 tiles)
     ldc     - the 1024^2 lid-driven cavity, 4 steps (50 Jacobi sweeps each)"""
@@ -998,6 +999,13 @@ def run_profile_2d(args):
             K = (dt * dt) * c * c
             uN = solver.forward(K, u0)
             solver.backward(K, (uN - target) * mask)
+        elif args.profile_op == "heat":
+            n, g = 256, 1
+            dx = 1.0 / n
+            u0 = torch.rand((n + 2, n + 2, 1, 1), device="cuda")
+            bc = P.GridBoundary(u0, dx, g)
+            bc.dirichlet_BC("ALL", 0.0)
+            P.HeatRollout(bc, dx, 1.0, 0.2 * dx * dx, steps_per_pass=8)(u0, 96)
         elif args.profile_op == "heatadj":
             n, g = 256, 1
             dx = 1.0 / n
