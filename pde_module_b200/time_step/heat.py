@@ -90,9 +90,16 @@ class HeatSolver:
         self.set_checkpoint_every(checkpoint_every)
 
     def set_checkpoint_every(self, every: int | None) -> None:
-        """Checkpoint spacing (None: ceil(sqrt(N))); frees the buffers and graphs."""
+        """Checkpoint spacing (None: ceil(sqrt(N)) rounded up to a multiple of the pass
+        depth, so no segment ends with a short pass); frees the buffers and graphs."""
         import math
-        self.every = int(every) if every else max(1, int(math.ceil(math.sqrt(self.N))))
+        self._every_auto = not every
+        if every:
+            self.every = int(every)
+        else:  # about sqrt(N), rounded up to whole passes of k steps (k = 8 when left to the library)
+            k = self._steps_per_pass if self._steps_per_pass > 0 else 8
+            e = max(1, int(math.ceil(math.sqrt(self.N))))
+            self.every = max(1, min(self.N, -(-e // k) * k))
         self.segments = [(n0, min(self.every, self.N - n0)) for n0 in range(0, self.N, self.every)]
         self._dev = None
         self._seq_f = GraphedSequence(self._run_forward, self.graphs)
@@ -105,8 +112,11 @@ class HeatSolver:
     @steps_per_pass.setter
     def steps_per_pass(self, k: int) -> None:
         self._steps_per_pass = int(k)
-        self._seq_f.reset()
-        self._seq_b.reset()
+        if self._every_auto:
+            self.set_checkpoint_every(None)  # the spacing follows the pass depth
+        else:
+            self._seq_f.reset()
+            self._seq_b.reset()
 
     def _buffers(self, like: torch.Tensor) -> None:
         if self._dev == like.device:
