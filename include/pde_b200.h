@@ -279,6 +279,32 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
                     const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
                     const PdeLDCParams* params, int32_t nsteps, void* stream);
 
+/* ---- weakly compressible flow, RK2 (new: the reference composes the step from
+ * its modules, examples/LDC/LDC_RK2.py) ----
+ * Parameters as the caller's doubles; each is rounded to fp32 as the module
+ * chain receives it (dt/2 is formed in double first). */
+typedef struct PdeWCParams {
+  double nu;    /* viscosity: Lap(u, nu)                      */
+  double eps;   /* biharmonic damping: Lap(Lap(u, nu), eps)   */
+  double c2;    /* sound speed squared: p = c2 * (rho - rho0) */
+  double rho0;  /* reference density                          */
+  double dt;    /* time step                                  */
+} PdeWCParams;
+
+/* nsteps RK2 (midpoint) steps of momentum m (X,Y,1,2) and density rho (X,Y,1,1),
+ * one fused launch per step, bit-identical to the composition of the reference
+ * operators (one rounding per product and sum, time_step/rungeKatta.py:123-174):
+ *   bc(m, rho) = (rho' * u', rho') with u = m / rho, u' = BC_u(u), rho' = BC_rho(rho)
+ *   f(m, rho)  = (((Grad(c2 (rho - rho0), -1) - Div(outer(m, u), 1)) + Lap(u, nu))
+ *                 + Lap(Lap(u, nu), eps),  Div(m, -1)),  u = m / rho
+ *   y0 = bc(y);  y1 = bc(y0 + (dt/2) f(y0));  y' = y0 + dt f(y1)
+ * (operator outputs 0 outside the array interior).  u_rules: 2 components,
+ * rho_rules: 1 (pde_bc_compile, constant face groups).  2D grids, order 2.
+ * work: 3 X Y floats.  m_out / rho_out may equal the inputs. */
+int pde_wc_rk2(const float* m_in, const float* rho_in, float* m_out, float* rho_out,
+               const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* rho_rules,
+               const PdeWCParams* params, int32_t nsteps, float* work, void* stream);
+
 /* One phase of a fractional step on a slab of the cavity: the rows
  * [x_offset, x_offset + grid->shape[0]) of a domain of x_global rows (grid
  * describes the slab's arrays; the other extents, ghost cells and dx are the

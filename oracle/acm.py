@@ -19,6 +19,10 @@ imports it.
 * RungeKatta1 / RungeKatta2 — time_step/rungeKatta.py:21-174, composed from the
   fdm oracle's GridBoundary, Laplacian and ForwardEuler (RungeKatta1 steps with
   dt / 2, as the reference does, :79-83).
+* The weakly compressible RK2 step of examples/LDC/LDC_RK2.py (bc and f at
+  :116-140: u = m/rho, boundary fills, momentum, divergence, Laplacian, outer
+  product, biharmonic damping, pressure gradient), composed of the operators
+  above, for the fused kernel's parity (its own operators pinned as above).
 
 The layer profile (dx / L) ** beta is a float32 power (the C library's powf, as
 the reference's CPU kernels and NumPy's float32 scalar power both call).
@@ -122,3 +126,41 @@ def runge_kutta(order: int, fields, groups, alphas, dx, ghost, dt, steps):
             ys = [fdm.forward_euler(y, k, dt) for y, k in zip(y0, k2)]
         t += dt
     return ys
+
+
+# ---- weakly compressible RK2 step (examples/LDC/LDC_RK2.py composed of the above) ----
+def wc_bc(m, rho, u_groups, rho_groups, dx, ghost):
+    """bc(t, m, rho) of LDC_RK2.py: u = m / rho; BC_u(u); BC_rho(rho); m = rho * u."""
+    u = (m / rho).astype(np.float32)
+    u = fdm.bc_apply(u, u_groups, dx, ghost)
+    r = fdm.bc_apply(rho, rho_groups, dx, ghost)
+    return scalar_mult(r, u), r
+
+
+def wc_f(m, rho, dx, ghost, nu, eps, c2, rho0):
+    """f(t, m, rho) of LDC_RK2.py (momentum and density rates)."""
+    u = (m / rho).astype(np.float32)
+    m_div = fdm.divergence(m, dx, ghost, -1.0)
+    u_diff = fdm.laplacian(u, dx, ghost, nu)
+    u_conv = fdm.divergence(outer(m, u), dx, ghost, 1.0)
+    u_damp = fdm.laplacian(u_diff, dx, ghost, eps)
+    p = (np.float32(c2) * (rho - np.float32(rho0))).astype(np.float32)
+    dp = fdm.grad(p, dx, ghost, -1.0)
+    k_m = (((dp - u_conv) + u_diff) + u_damp).astype(np.float32)
+    return k_m, m_div
+
+
+def wc_rk2(m, rho, u_groups, rho_groups, dx, ghost, nu, eps, c2, rho0, dt, nsteps):
+    """nsteps of RungeKatta2 (rungeKatta.py:123-174) with the bc and f above."""
+    m = np.asarray(m, dtype=np.float32)
+    rho = np.asarray(rho, dtype=np.float32)
+    for _ in range(nsteps):
+        m0, r0 = wc_bc(m, rho, u_groups, rho_groups, dx, ghost)
+        km, kr = wc_f(m0, r0, dx, ghost, nu, eps, c2, rho0)
+        m1 = fdm.forward_euler(m0, km, dt / 2)
+        r1 = fdm.forward_euler(r0, kr, dt / 2)
+        m1, r1 = wc_bc(m1, r1, u_groups, rho_groups, dx, ghost)
+        km, kr = wc_f(m1, r1, dx, ghost, nu, eps, c2, rho0)
+        m = fdm.forward_euler(m0, km, dt)
+        rho = fdm.forward_euler(r0, kr, dt)
+    return m, rho

@@ -11,11 +11,13 @@ from .FDM import (Laplacian, Grad, Divergence, GridBoundary, ImmersedBoundary, O
 from .time_step import (ForwardEuler, HeatRollout, HeatSolver, heat_rollout, FractionalStepLDC,
                         SlabFractionalStepLDC, WaveSolver,
                         wave_rollout,
-                        BatchedHeatRollout, BatchedWaveRollout, RungeKatta1, RungeKatta2)
+                        BatchedHeatRollout, BatchedWaveRollout, RungeKatta1, RungeKatta2,
+                        WeaklyCompressibleRK2, lid_driven_cavity_wc)
 from .mesh import UniformGridMesh, create_structured_field, create_structured_warp_field
 
 __all__ = ["Laplacian", "Grad", "Divergence", "GridBoundary", "ImmersedBoundary", "OuterProduct", "scalarVectorMult",
-           "FarField", "ViscousDampingLayer", "ForwardEuler", "RungeKatta1", "RungeKatta2", "HeatRollout",
+           "FarField", "ViscousDampingLayer", "ForwardEuler", "RungeKatta1", "RungeKatta2", "WeaklyCompressibleRK2",
+           "lid_driven_cavity_wc", "HeatRollout",
            "FractionalStepLDC", "SlabFractionalStepLDC",
            "HeatSolver", "heat_rollout", "WaveSolver", "wave_rollout", "BatchedHeatRollout", "BatchedWaveRollout",
            "UniformGridMesh", "create_structured_field", "create_structured_warp_field"]

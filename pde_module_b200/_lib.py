@@ -78,6 +78,11 @@ class PdeLDCParams(C.Structure):
     _fields_ = [("nu", C.c_float), ("dt", C.c_float), ("jacobi_iters", C.c_int32), ("jacobi_per_pass", C.c_int32)]
 
 
+class PdeWCParams(C.Structure):
+    _fields_ = [("nu", C.c_double), ("eps", C.c_double), ("c2", C.c_double), ("rho0", C.c_double),
+                ("dt", C.c_double)]
+
+
 class PdeBatchGrid(C.Structure):
     _fields_ = [("field", C.c_void_p), ("field_prev", C.c_void_p), ("scratch", C.c_void_p),
                 ("shape", C.c_int64 * 2), ("dx", C.c_double), ("coef", C.c_float), ("dt", C.c_float)]
@@ -136,6 +141,9 @@ _SIGS = {
     "pde_scalar_mult": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_void_p]),
     "pde_layer_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_float,
                                   C.c_void_p, C.c_void_p]),
+    "pde_wc_rk2": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid),
+                             C.POINTER(PdeBCRules), C.POINTER(PdeBCRules), C.POINTER(PdeWCParams), C.c_int32,
+                             C.c_void_p, C.c_void_p]),
     "pde_heat_rollout_at": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                       C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                       C.c_double, C.c_double, C.c_void_p]),

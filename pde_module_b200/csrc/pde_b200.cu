@@ -10,6 +10,7 @@
 #include "stream3d.cuh"
 #include "fused.cuh"
 #include "ldc.cuh"
+#include "wc.cuh"
 #include "wave.cuh"
 #include "batched.cuh"
 #include "heat_adj.cuh"
@@ -1098,6 +1099,76 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
     ldc_project_kernel<<<grid2, 256, 0, st>>>(u_star, p, u, G, *u_rules, *p_rules, K, 0);
     rc = launch_status();
     if (rc) return rc;
+  }
+  return PDE_OK;
+}
+
+int pde_wc_rk2(const float* m_in, const float* rho_in, float* m_out, float* rho_out, const PdeGrid* grid,
+               const PdeBCRules* u_rules, const PdeBCRules* rho_rules, const PdeWCParams* prm, int32_t nsteps,
+               float* work, void* stream) {
+  if (!m_in || !rho_in || !m_out || !rho_out || !grid || !u_rules || !rho_rules || !prm || !work || nsteps < 0)
+    return PDE_ERR_ARG;
+  if (work == m_in || work == m_out || work == rho_in || work == rho_out) return PDE_ERR_ARG;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  if (G.ndims != 2 || G.n[2] != 1 || grid->order != 2 || G.g < 1) return PDE_ERR_UNSUPPORTED;
+  if (G.n[0] < 2 * G.g + 3 || G.n[1] < 2 * G.g + 3) return PDE_ERR_SHAPE;
+  if (u_rules->ncomp != 2 || rho_rules->ncomp != 1 || u_rules->has_ramp || rho_rules->has_ramp) return PDE_ERR_ARG;
+  cudaStream_t st = as_stream(stream);
+  const size_t cells = (size_t)G.n[0] * G.n[1];
+  if (nsteps == 0) {
+    if (m_out != m_in) PDE_CUDA_CHECK(cudaMemcpyAsync(m_out, m_in, 2 * cells * 4, cudaMemcpyDeviceToDevice, st));
+    if (rho_out != rho_in) PDE_CUDA_CHECK(cudaMemcpyAsync(rho_out, rho_in, cells * 4, cudaMemcpyDeviceToDevice, st));
+    return PDE_OK;
+  }
+  WCParams P;
+  memset(&P, 0, sizeof(P));
+  P.X = (int)G.n[0];
+  P.Y = (int)G.n[1];
+  P.g = G.g;
+  int t = 32;
+  if ((long long)((P.X + 31) / 32) * ((P.Y + 31) / 32) < sm_count()) t = 16;  // small grids: more tiles
+  P.TBX = P.TBY = t;
+  if (g_tile2d[0] > 0) {  // pde_set_launch_2d
+    P.TBX = g_tile2d[0];
+    P.TBY = g_tile2d[1];
+  }
+  P.tiles_y = (P.Y + P.TBY - 1) / P.TBY;
+  P.RC = (P.TBX + 2 * WC_HALO) * (P.TBY + 2 * WC_HALO);
+  const size_t smem = (size_t)10 * P.RC * sizeof(float);
+  if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  const Weights WL = lap_weights(2, grid->dx), WD = d1_weights(2, grid->dx);
+  for (int i = 0; i < 3; ++i) {
+    P.wl[i] = WL.w[i];
+    P.wd[i] = WD.w[i];
+  }
+  P.nu = (float)prm->nu;
+  P.eps = (float)prm->eps;
+  P.c2 = (float)prm->c2;
+  P.rho0 = (float)prm->rho0;
+  P.dt_half = (float)(prm->dt / 2);
+  P.dt = (float)prm->dt;
+  PDE_CUDA_CHECK(cudaFuncSetAttribute(wc_rk2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
+  float* wm = work;
+  float* wr = work + 2 * cells;
+  const bool alias = m_out == m_in || rho_out == rho_in;
+  bool to_out = alias ? false : (nsteps % 2 == 1);
+  const float* sm_ = m_in;
+  const float* sr = rho_in;
+  for (int s = 0; s < nsteps; ++s) {
+    float* dm = to_out ? m_out : wm;
+    float* dr = to_out ? rho_out : wr;
+    wc_rk2_kernel<<<tiles, 256, smem, st>>>(sm_, sr, dm, dr, P, *u_rules, *rho_rules);
+    const int rc = launch_status();
+    if (rc) return rc;
+    sm_ = dm;
+    sr = dr;
+    to_out = !to_out;
+  }
+  if (sm_ != m_out) {
+    PDE_CUDA_CHECK(cudaMemcpyAsync(m_out, sm_, 2 * cells * 4, cudaMemcpyDeviceToDevice, st));
+    PDE_CUDA_CHECK(cudaMemcpyAsync(rho_out, sr, cells * 4, cudaMemcpyDeviceToDevice, st));
   }
   return PDE_OK;
 }

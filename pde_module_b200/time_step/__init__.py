@@ -4,3 +4,4 @@ from .fractional_step import FractionalStepLDC, SlabFractionalStepLDC
 from .wave import WaveSolver, wave_rollout
 from .batched import BatchedHeatRollout, BatchedWaveRollout
 from .rungeKatta import RungeKatta1, RungeKatta2, SignatureMismatchError
+from .weakly_compressible import WeaklyCompressibleRK2, lid_driven_cavity_wc
