@@ -418,6 +418,9 @@ def run_ours(args):
     wave = None
     if world == 1 and not args.no_wave:  # a single-GPU workload (replicas only): not run beside other ranks
         wave = run_wave()
+    wc = None
+    if world == 1 and not args.no_wc:  # a single-GPU workload (replicas only): not run beside other ranks
+        wc = run_wc()
     batched = None
     if world == 1 and not args.no_batched:  # a single-GPU workload (replicas only): not run beside other ranks
         batched = run_batched(tune=not args.no_tune)
@@ -448,6 +451,7 @@ def run_ours(args):
             "ldc_1024": ldc,
             "wave_512": wave,
             "batched_64": batched,
+            "wc_cavity": wc,
             "autotune": {f"{k[0]}_n{k[1]}_o{k[2]}": v for k, v in tuned.items()},
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * len(ops), "clocks": clocks,
@@ -762,6 +766,81 @@ def batched_problem(n_grids: int = 64, lo: int = 64, hi: int = 1024):
     return sides, alpha.tolist(), u0, dx, dt
 
 
+def run_wc(sizes=(201, 1025), steps: int = 100, chain_steps: int = 10):
+    """Weakly compressible cavity (examples/LDC/LDC_RK2.py): n x n nodes, RK2 steps
+    as one fused launch each (pde_wc_rk2) against the same step composed of this
+    package's modules (GridBoundary, Laplacian, Grad, Divergence, OuterProduct,
+    scalarVectorMult, RungeKatta2, torch arithmetic for the map-wise lines), both
+    replayed as CUDA graphs; checks the two agree bit for bit."""
+    import torch
+    import pde_module_b200 as P
+
+    def graph_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s):
+                fn()
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"workload": "weakly compressible lid-driven cavity (LDC_RK2.py: Re 100, M 0.1, CFL 0.8), RK2 steps"}
+    for n in sizes:
+        solver, m, rho = P.lid_driven_cavity_wc(n=n)
+        dx, nu, c2 = 1.0 / (n - 1), 0.01, 100.0
+        eps, dt = solver.params.eps, solver.dt
+        u_bc = P.GridBoundary(m, dx, 1)
+        u_bc.dirichlet_BC("ALL", 0.0)
+        u_bc.dirichlet_BC("+Y", 1.0, 0)
+        r_bc = P.GridBoundary(rho, dx, 1)
+        r_bc.vonNeumann_BC("ALL", 0.0)
+        lap_u, lap_d = P.Laplacian(2, dx, 1), P.Laplacian(2, dx, 1)
+        div_m, div_t = P.Divergence(2, m.shape, dx, 1), P.Divergence((2, 2), m.shape, dx, 1)
+        grad_p, outer, momentum = P.Grad(1, rho.shape, dx, 1), P.OuterProduct(2, 2), P.scalarVectorMult(2)
+
+        def bc(t, m_, r_):
+            r2 = r_bc(r_)
+            return momentum(r2, u_bc(m_ / r_)), r2
+
+        def f(t, m_, r_):
+            u = m_ / r_
+            u_diff = lap_u(u, nu)
+            return (grad_p(c2 * (r_ - 1.0), -1.0) - div_t(outer(m_, u)) + u_diff + lap_d(u_diff, eps),
+                    div_m(m_, -1.0))
+
+        rk = P.RungeKatta2([2, 1], f=f, bc=bc)
+        m0 = m + 0.01 * torch.rand_like(m)
+        state = [m0.clone(), rho.clone()]
+
+        def chain():
+            a, b = state
+            for _ in range(chain_steps):
+                a, b = rk(0.0, dt, a, b)
+            state[0], state[1] = a, b
+
+        fused_ms = graph_ms(lambda: solver(m0, rho, steps)) / steps
+        chain_ms = graph_ms(chain) / chain_steps
+        a, b = rk(0.0, dt, m0, rho)
+        fm, fr = solver(m0, rho, 1)
+        cells = n * n  # the nodes (the operators' launch domain)
+        out[f"n{n}"] = {"fused_ms_per_step": round(fused_ms, 5), "chain_ms_per_step": round(chain_ms, 5),
+                        "speedup": round(chain_ms / fused_ms, 2),
+                        "fused_cell_updates_per_s": cells / (fused_ms / 1000.0),
+                        "bitwise_equal_to_chain": bool(torch.equal(a, fm) and torch.equal(b, fr))}
+    return out
+
+
 def run_batched(steps: int = 500, chain_steps: int = 50, tune: bool = True):
     """Batched heat and wave rollouts of 64 uneven grids in one persistent launch
     (replayed as a CUDA graph), against per-grid plain launches: the module chain
@@ -1042,6 +1121,7 @@ def main():
     ap.add_argument("--no-ldc", action="store_true")
     ap.add_argument("--no-wave", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-wc", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the library's default tile candidates")
     ap.add_argument("--profile-op", default=None, help="run one operator only (lap2, grad4, div2, ...)")
     ap.add_argument("--profile-n", type=int, default=N_INT)
