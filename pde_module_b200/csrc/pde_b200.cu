@@ -1126,13 +1126,17 @@ int pde_wc_rk2(const float* m_in, const float* rho_in, float* m_out, float* rho_
   P.X = (int)G.n[0];
   P.Y = (int)G.n[1];
   P.g = G.g;
-  int t = 32;
-  if ((long long)((P.X + 31) / 32) * ((P.Y + 31) / 32) < sm_count()) t = 16;  // small grids: more tiles
-  P.TBX = P.TBY = t;
+  // automatic shape: 32x32 tiles; 16x16 when those leave SMs idle, 64x32 when
+  // there are several per SM (fewer halo cells per tile cell)
+  const long long t32 = (long long)((P.X + 31) / 32) * ((P.Y + 31) / 32);
+  P.TBX = P.TBY = 32;
+  if (t32 < sm_count()) P.TBX = P.TBY = 16;
+  else if (t32 >= 4LL * sm_count()) P.TBX = 64;
   if (g_tile2d[0] > 0) {  // pde_set_launch_2d
     P.TBX = g_tile2d[0];
     P.TBY = g_tile2d[1];
   }
+  const int threads = (g_threads2d == 256 || g_threads2d == 512) ? g_threads2d : 512;
   P.tiles_y = (P.Y + P.TBY - 1) / P.TBY;
   P.RC = (P.TBX + 2 * WC_HALO) * (P.TBY + 2 * WC_HALO);
   const size_t smem = (size_t)10 * P.RC * sizeof(float);
@@ -1159,7 +1163,7 @@ int pde_wc_rk2(const float* m_in, const float* rho_in, float* m_out, float* rho_
   for (int s = 0; s < nsteps; ++s) {
     float* dm = to_out ? m_out : wm;
     float* dr = to_out ? rho_out : wr;
-    wc_rk2_kernel<<<tiles, 256, smem, st>>>(sm_, sr, dm, dr, P, *u_rules, *rho_rules);
+    wc_rk2_kernel<<<tiles, threads, smem, st>>>(sm_, sr, dm, dr, P, *u_rules, *rho_rules);
     const int rc = launch_status();
     if (rc) return rc;
     sm_ = dm;

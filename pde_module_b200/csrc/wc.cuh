@@ -43,7 +43,7 @@ __device__ __forceinline__ void wc_region(int RC, int RY, F fn) {
   for (int i = threadIdx.x; i < RC; i += blockDim.x, wk.next()) fn(i, wk.row, wk.col);
 }
 
-__global__ void __launch_bounds__(256) wc_rk2_kernel(const float* __restrict__ m_in, const float* __restrict__ r_in,
+__global__ void __launch_bounds__(512) wc_rk2_kernel(const float* __restrict__ m_in, const float* __restrict__ r_in,
                                                      float* __restrict__ m_out, float* __restrict__ r_out,
                                                      const WCParams P, const PdeBCRules Ru, const PdeBCRules Rr) {
   extern __shared__ __align__(16) float sm[];
