@@ -617,12 +617,13 @@ def run_ldc(steps: int = 2000, n: int = 1024):
 
     import pde_module_b200._lib as L
     tune = {}
-    for tile in ((0, 0), (32, 64), (64, 64), (48, 96), (32, 128)):
-        L.check(L.lib().pde_set_launch_2d(tile[0], tile[1], 0), "pde_set_launch_2d")
+    for tile in ((0, 0, 0), (32, 64, 0), (64, 64, 0), (64, 64, 512), (64, 64, 1024), (48, 96, 0), (48, 96, 512),
+                 (32, 128, 0), (32, 128, 512)):
+        L.check(L.lib().pde_set_launch_2d(*tile), "pde_set_launch_2d")
         for kk in (5, 8, 10, 16):
             tune[(tile, kk)] = timed_rollout(kk, 40)
     tile, k = min(tune, key=tune.get)
-    L.check(L.lib().pde_set_launch_2d(tile[0], tile[1], 0), "pde_set_launch_2d")
+    L.check(L.lib().pde_set_launch_2d(*tile), "pde_set_launch_2d")
     ms = timed_rollout(k, steps)
     L.check(L.lib().pde_set_launch_2d(0, 0, 0), "pde_set_launch_2d")
     u = s.u.cpu().numpy()
@@ -631,8 +632,8 @@ def run_ldc(steps: int = 2000, n: int = 1024):
                         f"{steps} steps from rest, dt {s.dt:.3e}",
             "ms": ms, "cell_updates_per_s": cells / (ms / 1000.0),
             "jacobi_sweeps_per_s": 50 * steps / (ms / 1000.0), "jacobi_per_pass": k,
-            "jacobi_tile": list(tile) if tile != (0, 0) else "auto",
-            "tune_ms_40_steps": {f"{t[0]}x{t[1]}_k{kk}": round(v, 3) for (t, kk), v in tune.items()},
+            "jacobi_launch": list(tile) if tile != (0, 0, 0) else "auto",
+            "tune_ms_40_steps": {f"{t[0]}x{t[1]}t{t[2]}_k{kk}": round(v, 3) for (t, kk), v in tune.items()},
             "launches_per_step": 3 + -(-50 // k) + (1 if (-(-50 // k)) % 2 else 0),
             "max_abs_u": float(np.abs(u).max()),
             "note": "L2-resident (about 28 MB of fields); CUDA graph replay of the whole rollout"}

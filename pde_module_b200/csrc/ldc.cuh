@@ -178,7 +178,7 @@ struct J2Params {
   int last;  // this pass ends the step's sweeps: accumulate the residual
 };
 
-__global__ void __launch_bounds__(256) jacobi2d_tb_kernel(const float* __restrict__ pin, float* __restrict__ pout,
+__global__ void __launch_bounds__(1024) jacobi2d_tb_kernel(const float* __restrict__ pin, float* __restrict__ pout,
                                                            const float* __restrict__ rhs, float* __restrict__ resid,
                                                            const J2Params P, const PdeBCRules Rp) {
   extern __shared__ __align__(16) float sm[];

@@ -1090,7 +1090,8 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
       JP.k = (iters - done < k) ? (iters - done) : k;
       done += JP.k;
       JP.last = (done == iters);
-      jacobi2d_tb_kernel<<<jtiles, 256, jsmem, st>>>(src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
+      jacobi2d_tb_kernel<<<jtiles, g_threads2d > 0 ? g_threads2d : 256, jsmem, st>>>(
+          src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
       float* t = src;
       src = dst;
       dst = t;
@@ -1234,7 +1235,7 @@ int pde_ldc_slab_step(int32_t phase, float* u, float* u_star, const float* p_in,
       if (rc) return rc;
       JP.k = nsweeps;
       JP.last = last ? 1 : 0;
-      jacobi2d_tb_kernel<<<jtiles, 256, jsmem, st>>>(gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1),
+      jacobi2d_tb_kernel<<<jtiles, g_threads2d > 0 ? g_threads2d : 256, jsmem, st>>>(gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1),
                                                      resid, JP, *p_rules);
       break;
     }
