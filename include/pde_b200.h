@@ -365,16 +365,17 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
                   float* lstates_fwd, const float* mu_next, const float* mu_next2, float* mu_out, float* mu_out_next,
                   const float* lstates_adj, float* grad_K, int32_t nsteps_adj, const float* src, int64_t src_cell,
                   int32_t steps_per_pass, float* work, const PdeGrid* grid, void* stream);
-/* Launch shape of the temporally blocked 2D kernels of pde_heat_rollout[_at],
+/* Launch shape of the tiled 2D kernels of pde_heat_rollout[_at],
  * pde_heat_forward, pde_heat_adjoint, pde_wave_forward, pde_wave_adjoint,
- * pde_wave_pair and the Jacobi sweeps of pde_ldc_rollout, process-wide:
+ * pde_wave_pair, pde_wc_rk2 and the Jacobi sweeps of pde_ldc_rollout and
+ * pde_ldc_slab_step, process-wide:
  * output tile (sides 8..256; (0, 0) = automatic: the largest of 32x64, 32x32,
  * 16x32 that gives every SM a tile, enlarged slightly when the count is just
  * above a multiple of the SM count; for the fused heat rollout square tiles of
  * about one per SM, sides 16..64) and threads per block (256, 512, 1024;
  * 0 = automatic: for the wave and differentiable-heat kernels 1024 with up to one
- * tile per SM, 512 up to two, else 256; 512 for the fused heat rollout; the Jacobi
- * sweeps use 256). */
+ * tile per SM, 512 up to two, else 256; 512 for the fused heat rollout and the
+ * weakly compressible step (which takes 256 or 512); 256 for the Jacobi sweeps). */
 int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads);
 
 /* ---- batched rollouts (new: the reference advances every grid with its own
