@@ -145,6 +145,9 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
                        ? (P.srcx - rx0) * RY + (P.srcy - ry0) : -1;
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, P.Y);
+    float kc[MAXC];  // K of the thread's cells (constant over the pass)
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) kc[c] = C.ri[c] >= 0 ? sm[ok + C.ri[c]] : 0.0f;
     for (int s = 0; s < P.k; ++s) {
       const float sn = (srci >= 0) ? P.src[P.n0 + s] : 0.0f;
       float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
@@ -154,7 +157,7 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
         if (i < 0) continue;
         const float lap = lap5s(sm, o0 + i, RY, P.w);
         float v = sub(mul(2.0f, sm[o0 + i]), sm[om + i]);
-        v = add(v, mul(sm[ok + i], lap));
+        v = add(v, mul(kc[c], lap));
         if (i == srci) v = add(v, sn);
         sm[op + i] = v;
         if (STORE && C.gi[c] >= 0) Ls[C.gi[c]] = lap;
@@ -252,12 +255,13 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
   const WaveRect Rt(P, Rg);
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, P.Y);
-    float ga[MAXC], lnext[MAXC];
+    float ga[MAXC], lnext[MAXC], kc[MAXC];
     const float* L0 = P.lsts + (size_t)P.ntop * P.cells;
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
       ga[c] = C.gi[c] >= 0 ? P.gK[C.gi[c]] : 0.0f;
       lnext[c] = C.gi[c] >= 0 ? __ldg(L0 + C.gi[c]) : 0.0f;
+      kc[c] = C.ri[c] >= 0 ? sm[okk + C.ri[c]] : 0.0f;  // K of the thread's cells
     }
     for (int s = 0; s < P.k; ++s) {
       float ln[MAXC];
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
         const float acc = lap5s(sm, k1 + i, RY, P.w);
         const float v = add(sub(mul(2.0f, m1), sm[o2 + i]), acc);
         sm[o0 + i] = v;
-        sm[k0 + i] = mul(sm[okk + i], v);
+        sm[k0 + i] = mul(kc[c], v);
       }
       __syncthreads();
       const int t = o2;
@@ -389,11 +393,12 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
                        ? (Pf.srcx - rx0) * RY + (Pf.srcy - ry0) : -1;
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, Pa.Y);
-    float ga[MAXC], lnext[MAXC];
+    float ga[MAXC], lnext[MAXC], kc[MAXC];
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
       ga[c] = 0.0f;
       lnext[c] = 0.0f;
+      kc[c] = C.ri[c] >= 0 ? sm[okk + C.ri[c]] : 0.0f;  // K of the thread's cells, for both chains
       if (adj && C.gi[c] >= 0) {
         ga[c] = Pa.gK[C.gi[c]];
         lnext[c] = __ldg(Pa.lsts + (size_t)Pa.ntop * Pa.cells + C.gi[c]);
@@ -419,7 +424,7 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
         if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
           const float lap = lap5s(sm, f0 + i, RY, Pf.w);
           float v = sub(mul(2.0f, sm[f0 + i]), sm[fm + i]);
-          v = add(v, mul(sm[okk + i], lap));
+          v = add(v, mul(kc[c], lap));
           if (i == srci) v = add(v, sn);
           sm[fp + i] = v;
           if (C.gi[c] >= 0) Ls[C.gi[c]] = lap;
@@ -431,7 +436,7 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
           const float acc = lap5s(sm, k1 + i, RY, Pa.w);
           const float v = add(sub(mul(2.0f, m1), sm[a2 + i]), acc);
           sm[a0 + i] = v;
-          sm[k0 + i] = mul(sm[okk + i], v);
+          sm[k0 + i] = mul(kc[c], v);
         }
       }
       __syncthreads();
