@@ -83,10 +83,14 @@ struct WaveRect {
 // c < MAXC: the same cells in every step (the rectangle is fixed for the pass),
 // so their indices, the gradient sums of the tile cells among them and the next
 // step's L(u^n) values stay in registers.  Needs count <= MAXC * blockDim.x.
+// dist: the cell's distance from the tile (the larger of its x and y distances).
+// Step s of a k-step pass only has to update cells with dist <= k - 1 - s: the
+// tile's values after the pass depend on no other cell, so the rest is skipped.
 template <int MAXC>
 struct WaveCells {
-  int ri[MAXC];  // region index; -1 past the rectangle
-  int gi[MAXC];  // array index of a tile cell; -1 for the other cells
+  int ri[MAXC];    // region index; -1 past the rectangle
+  int gi[MAXC];    // array index of a tile cell; -1 for the other cells
+  int dist[MAXC];  // distance from the tile
   __device__ WaveCells(const WaveRect& Rt, const WaveRegion& Rg, int Y) {
     const int nt = (int)blockDim.x;
     const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
@@ -95,10 +99,12 @@ struct WaveCells {
     for (int c = 0; c < MAXC; ++c) {
       ri[c] = -1;
       gi[c] = -1;
+      dist[c] = 1 << 20;
       if ((int)threadIdx.x + c * nt < Rt.count) {
         ri[c] = (Rt.cx0 + wk.row) * Rg.RY + Rt.cy0 + wk.col;
         const int ox = wk.row - tx0, oy = wk.col - ty0;
         if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) gi[c] = (Rg.bx0 + ox) * Y + Rg.by0 + oy;
+        dist[c] = max(max(max(-ox, ox - (Rg.OX - 1)), max(-oy, oy - (Rg.OY - 1))), 0);
       }
       wk.next();
     }
@@ -151,10 +157,11 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
     for (int s = 0; s < P.k; ++s) {
       const float sn = (srci >= 0) ? P.src[P.n0 + s] : 0.0f;
       float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
+      const int reach = P.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
         const int i = C.ri[c];
-        if (i < 0) continue;
+        if (i < 0 || C.dist[c] > reach) continue;
         const float lap = lap5s(sm, o0 + i, RY, P.w);
         float v = sub(mul(2.0f, sm[o0 + i]), sm[om + i]);
         v = add(v, mul(kc[c], lap));
@@ -273,10 +280,11 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
         for (int c = 0; c < MAXC; ++c)
           if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
       }
+      const int reach = P.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
         const int i = C.ri[c];
-        if (i < 0) continue;
+        if (i < 0 || C.dist[c] > reach) continue;
         const float m1 = sm[o1 + i];
         if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
         const float acc = lap5s(sm, k1 + i, RY, P.w);
@@ -417,11 +425,12 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
         for (int c = 0; c < MAXC; ++c)
           if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
       }
+      const int freach = Pf.k - 1 - s, areach = Pa.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
         const int i = C.ri[c];
         if (i < 0) continue;
-        if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+        if (fs && C.dist[c] <= freach) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
           const float lap = lap5s(sm, f0 + i, RY, Pf.w);
           float v = sub(mul(2.0f, sm[f0 + i]), sm[fm + i]);
           v = add(v, mul(kc[c], lap));
@@ -429,7 +438,7 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
           sm[fp + i] = v;
           if (C.gi[c] >= 0) Ls[C.gi[c]] = lap;
         }
-        if (as) {
+        if (as && C.dist[c] <= areach) {
           const float m1 = sm[a1 + i];
           if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
           // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
