@@ -817,11 +817,12 @@ bool wave_setup(const PdeGrid* grid, int steps_per_pass, int nsteps, Geo* G, Wav
   return *smem <= 227 * 1024;
 }
 
-// Register cell lists of the wave adjoint kernels: the region capacity bounds
-// every block's rectangle, so MAXC cells per thread cover it; 0 = the general
-// loop (rectangles beyond 8 cells per thread).
+// Register cell lists of the wave kernels: the region capacity bounds every
+// block's rectangle, so MAXC (4, 6 or 8) cells per thread cover it; 0 = the
+// general loop (rectangles beyond 8 cells per thread).
 int wave_cells_per_thread(int rc, int threads) {
   if (rc <= 4 * threads) return 4;
+  if (rc <= 6 * threads) return 6;
   if (rc <= 8 * threads) return 8;
   return 0;
 }
@@ -854,7 +855,7 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
   const int threads = pick_threads_2d(tiles);
   const int cpt = wave_cells_per_thread(P.RC, threads);
-  auto kern = cpt == 4 ? wave_fwd_tb_kernel<4> : cpt == 8 ? wave_fwd_tb_kernel<8> : wave_fwd_tb_kernel<0>;
+  auto kern = cpt == 4 ? wave_fwd_tb_kernel<4> : cpt == 6 ? wave_fwd_tb_kernel<6> : cpt == 8 ? wave_fwd_tb_kernel<8> : wave_fwd_tb_kernel<0>;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int npasses = (nsteps + k - 1) / k;
   float* w0 = work;
@@ -920,7 +921,7 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
   const int tiles = ((Pa.X + Pa.TBX - 1) / Pa.TBX) * Pa.tiles_y;
   const int threads = pick_threads_2d(tiles);
   const int cpt = wave_cells_per_thread(Pa.RC, threads);
-  auto kern = cpt == 4 ? wave_pair_tb_kernel<4> : cpt == 8 ? wave_pair_tb_kernel<8> : wave_pair_tb_kernel<0>;
+  auto kern = cpt == 4 ? wave_pair_tb_kernel<4> : cpt == 6 ? wave_pair_tb_kernel<6> : cpt == 8 ? wave_pair_tb_kernel<8> : wave_pair_tb_kernel<0>;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   float* w[6];
   for (int i = 0; i < 6; ++i) w[i] = work + (size_t)i * Pa.cells;
@@ -982,7 +983,7 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
   const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
   const int threads = pick_threads_2d(tiles);
   const int cpt = wave_cells_per_thread(P.RC, threads);
-  auto kern = cpt == 4 ? wave_adj_tb_kernel<4> : cpt == 8 ? wave_adj_tb_kernel<8> : wave_adj_tb_kernel<0>;
+  auto kern = cpt == 4 ? wave_adj_tb_kernel<4> : cpt == 6 ? wave_adj_tb_kernel<6> : cpt == 8 ? wave_adj_tb_kernel<8> : wave_adj_tb_kernel<0>;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int npasses = (nsteps + k - 1) / k;
   float* w0 = work;
