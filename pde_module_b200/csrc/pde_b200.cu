@@ -197,7 +197,7 @@ int launch_candidate(int cand, const float* in, float* out, const Geo& G, const 
   } else if constexpr (OP == OP_GRAD) {
     switch (cand) {
       case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
-      case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 2: return launch_stream3d_k<R, OP, 1, 128, 8, 4, 6, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 3: return launch_stream3d_k<R, OP, 1, 128, 8, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       default: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 6, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
     }
