@@ -260,6 +260,9 @@ __global__ void __launch_bounds__(1024) heat2d_tb_kernel(const float* __restrict
   // stencil cells whose R neighbours along both axes are inside the region
   const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(P.X - g, rx0 + RX - R) - rx0;
   const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(P.Y - g, ry0 + RY - R) - ry0;
+  const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
+  // the tile in region coordinates (inclusive bounds)
+  const int tlx0 = bx0 - rx0, tlx1 = ox1 - 1 - rx0, tly0 = by0 - ry0, tly1 = oy1 - 1 - ry0;
   for (int s = 0; s < P.k; ++s) {
     if constexpr (RAMP) {
       // every read of SR's values in the previous step came before its last barrier
@@ -273,9 +276,17 @@ __global__ void __launch_bounds__(1024) heat2d_tb_kernel(const float* __restrict
     } else {
       bc_fill_region<N>(A, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
     }
-    RectWalk wk(nrow, nt);
-    for (int idx = threadIdx.x; idx < RF; idx += nt, wk.next()) {
-      const int lx = wk.row, ly = wk.col / N;
+    // Only the box of cells within R (k - 1 - s) + 1 of the tile can reach the
+    // tile's result (the boundary fills read inward, never farther out): the
+    // step walks that box; the cells outside it keep stale values nobody reads.
+    const int reach = R * (P.k - 1 - s) + 1;
+    const int bx_lo = max(tlx0 - reach, 0), bx_hi = min(tlx1 + reach, RX - 1);
+    const int by_lo = max(tly0 - reach, 0), by_hi = min(tly1 + reach, RY - 1);
+    const int bw = (by_hi - by_lo + 1) * N, bcount = (bx_hi - bx_lo + 1) * bw;
+    RectWalk wk(bw, nt);
+    for (int q = threadIdx.x; q < bcount; q += nt, wk.next()) {
+      const int lx = bx_lo + wk.row, lf = by_lo * N + wk.col, ly = lf / N;
+      const int idx = lx * nrow + lf;
       const float u2 = A[idx];
       float res = u2;
       if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) {
@@ -295,7 +306,6 @@ __global__ void __launch_bounds__(1024) heat2d_tb_kernel(const float* __restrict
   }
   // The ghost cells of the result hold the last step's boundary-filled values
   // (non-stencil cells copy their filled value through).
-  const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
   const int onrow = (oy1 - by0) * N;
   RectWalk wo(onrow, nt);
   for (int i = threadIdx.x; i < (ox1 - bx0) * onrow; i += nt, wo.next())

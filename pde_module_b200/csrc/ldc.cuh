@@ -213,18 +213,23 @@ __global__ void __launch_bounds__(1024) jacobi2d_tb_kernel(const float* __restri
   // stencil rectangle: cells of [g, n-g) whose four neighbours are inside the region
   const int sx0 = max(g, rx0 + 1) - rx0, sx1 = min(P.X - g, rx0 + RX - 1) - rx0;
   const int sy0 = max(g, ry0 + 1) - ry0, sy1 = min(P.Y - g, ry0 + RY - 1) - ry0;
-  const int SW = max(sy1 - sy0, 1), SC = max(sx1 - sx0, 0) * max(sy1 - sy0, 0);
-  const int dq = nt / SW, dr = nt - dq * SW;
-  // the tile in rectangle coordinates (residual cells)
-  const int tx0 = bx0 - rx0 - sx0, ty0 = by0 - ry0 - sy0;
   const int tw = min(bx0 + P.TBX, P.own_hi) - bx0, th = min(by0 + P.TBY, P.Y) - by0;
   float sq = 0.0f;
   for (int s = 0; s < P.k; ++s) {
     bc_fill_region<1>(A, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);
     const bool acc_res = P.last && s == P.k - 1;
+    // Sweep s only has to update the stencil cells within (k - 1 - s) + 1 of the
+    // tile (the boundary fills read inward): the stencil rectangle cut to that box.
+    const int reach = P.k - s;
+    const int qx0 = max(sx0, bx0 - rx0 - reach), qx1 = min(sx1, bx0 - rx0 + tw + reach);
+    const int qy0 = max(sy0, by0 - ry0 - reach), qy1 = min(sy1, by0 - ry0 + th + reach);
+    const int SW = max(qy1 - qy0, 1), SC = max(qx1 - qx0, 0) * max(qy1 - qy0, 0);
+    const int dq = nt / SW, dr = nt - dq * SW;
+    // the tile in box coordinates (residual cells)
+    const int tx0 = bx0 - rx0 - qx0, ty0 = by0 - ry0 - qy0;
     int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
     for (int c = threadIdx.x; c < SC; c += nt) {
-      const int i = (sx0 + lx) * RY + sy0 + ly;
+      const int i = (qx0 + lx) * RY + qy0 + ly;
       const float old = A[i];
       const float sum = add(add(add(A[i - RY], A[i + RY]), A[i - 1]), A[i + 1]);
       const float res = mul(0.25f, sub(sum, mul(P.h2, Rh[i])));
