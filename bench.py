@@ -1062,7 +1062,7 @@ def run_profile_op(args):
 
 def run_profile_2d(args):
     """The 2D time-stepping kernels for profilers, eager (no graphs), short runs:
-    wave    - 512^2 wave problem, 96 steps, forward + adjoint (k = 4, automatic tile)
+    wave    - 512^2 wave problem, 96 steps, forward + adjoint (k = 8, automatic tile)
     heat    - 256^2 fused heat rollout (Dirichlet 0), 96 steps (k = 8, automatic launch shape)
     heatadj - 256^2 heat, alpha field, 96 steps, forward + adjoint (k = 4)
     batched - the 64-grid batched heat rollout, 16 steps (k = 4, 64 x 64 tiles)
@@ -1073,7 +1073,7 @@ def run_profile_2d(args):
     t0 = time.time()
     for _ in range(args.iters):
         if args.profile_op == "wave":
-            solver, c, u0, target, dt, mask = W.make_problem(n=512, nsteps=96, steps_per_pass=4)
+            solver, c, u0, target, dt, mask = W.make_problem(n=512, nsteps=96, steps_per_pass=8)
             solver.graphs = False
             solver.set_checkpoint_every(None)
             K = (dt * dt) * c * c

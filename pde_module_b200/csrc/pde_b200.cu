@@ -838,7 +838,7 @@ int pde_wave_forward(const float* K, const float* u_prev, const float* u_cur, fl
   WaveParams P;
   int k;
   size_t smem;
-  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 4, 0)) return PDE_ERR_UNSUPPORTED;
+  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 3, 0)) return PDE_ERR_UNSUPPORTED;
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)P.cells;
   if (nsteps == 0) {
@@ -902,10 +902,10 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
   int k;
   size_t smem;
   // results do not depend on the pass depth: take the deepest one (up to the
-  // requested) whose nine region buffers fit in shared memory
+  // requested) whose seven interleaved region floats per cell fit in shared memory
   bool ok = false;
   for (int kk = steps_per_pass > 0 ? steps_per_pass : 8; kk >= 1 && !ok; --kk)
-    ok = wave_setup(grid, kk, nmax, &G, &Pa, &k, &smem, 9, 1);
+    ok = wave_setup(grid, kk, nmax, &G, &Pa, &k, &smem, 7, 1);
   if (!ok) return PDE_ERR_UNSUPPORTED;
   if (src_cell >= Pa.cells) return PDE_ERR_ARG;
   WaveParams Pf = Pa;
@@ -976,7 +976,7 @@ int pde_wave_adjoint(const float* K, const float* mu_next, const float* mu_next2
   WaveParams P;
   int k;
   size_t smem;
-  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 6, 1)) return PDE_ERR_UNSUPPORTED;
+  if (!wave_setup(grid, steps_per_pass, nsteps, &G, &P, &k, &smem, 5, 1)) return PDE_ERR_UNSUPPORTED;
 
   cudaStream_t st = as_stream(stream);
   const size_t bytes = sizeof(float) * (size_t)P.cells;

@@ -20,6 +20,8 @@
 // neighbour reads) and accumulates dJ/dK of its tile in shared memory, in the
 // order n = N-1 .. 0, so the result does not depend on k or the tile.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace pde {
@@ -68,40 +70,47 @@ struct WaveRegion {
 // cell inward per step.  Tile cells inside the ring are at least k cells from
 // any cut edge, so they always lie in the rectangle.
 struct WaveRect {
-  int cx0, cy0, W, count;
+  int cx0, cy0, W, NR, count;  // NR rows of W cells
   __device__ WaveRect(const WaveParams& P, const WaveRegion& Rg) {
     cx0 = max(P.g + 1, Rg.rx0 + 1) - Rg.rx0;
     const int cx1 = min(P.X - 1 - P.g, Rg.rx0 + Rg.RX - 1) - Rg.rx0;
     cy0 = max(P.g + 1, Rg.ry0 + 1) - Rg.ry0;
     const int cy1 = min(P.Y - 1 - P.g, Rg.ry0 + Rg.RY - 1) - Rg.ry0;
     W = max(cy1 - cy0, 0);
-    count = max(cx1 - cx0, 0) * W;
+    NR = max(cx1 - cx0, 0);
+    count = NR * W;
   }
 };
 
-// The rectangle cells of this thread, q = threadIdx.x + c * blockDim.x for
-// c < MAXC: the same cells in every step (the rectangle is fixed for the pass),
-// so their indices, the gradient sums of the tile cells among them and the next
-// step's L(u^n) values stay in registers.  Needs count <= MAXC * blockDim.x.
+// The rectangle cells of this thread: its slots q = threadIdx.x + c * blockDim.x
+// (c < MAXC) walk the rectangle's rows at their full region width RY, the
+// columns outside the rectangle left idle, so a warp's 32 slots are 32
+// consecutive region cells (NB-float stride in shared memory: no bank
+// conflicts) and no warp straddles the gap between two rectangle rows.  The
+// same cells in every step (the rectangle is fixed for the pass), so their
+// indices, the gradient sums of the tile cells among them and the next step's
+// L(u^n) values stay in registers.  Needs NR * RY <= MAXC * blockDim.x.
 // dist: the cell's distance from the tile (the larger of its x and y distances).
 // Step s of a k-step pass only has to update cells with dist <= k - 1 - s: the
 // tile's values after the pass depend on no other cell, so the rest is skipped.
 template <int MAXC>
 struct WaveCells {
-  int ri[MAXC];    // region index; -1 past the rectangle
+  int ri[MAXC];    // region index; -1 for an idle slot
   int gi[MAXC];    // array index of a tile cell; -1 for the other cells
-  int dist[MAXC];  // distance from the tile
+  int dist[MAXC];  // distance from the tile; 1 << 20 for an idle slot
   __device__ WaveCells(const WaveRect& Rt, const WaveRegion& Rg, int Y) {
     const int nt = (int)blockDim.x;
-    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
-    RectWalk wk(Rt.W, nt);
+    // tile origin: rows relative to the rectangle, columns relative to the region
+    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0;
+    const int n = Rt.NR * Rg.RY;
+    RectWalk wk(Rg.RY, nt);
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
       ri[c] = -1;
       gi[c] = -1;
       dist[c] = 1 << 20;
-      if ((int)threadIdx.x + c * nt < Rt.count) {
-        ri[c] = (Rt.cx0 + wk.row) * Rg.RY + Rt.cy0 + wk.col;
+      if ((int)threadIdx.x + c * nt < n && wk.col >= Rt.cy0 && wk.col < Rt.cy0 + Rt.W) {
+        ri[c] = (Rt.cx0 + wk.row) * Rg.RY + wk.col;
         const int ox = wk.row - tx0, oy = wk.col - ty0;
         if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) gi[c] = (Rg.bx0 + ox) * Y + Rg.by0 + oy;
         dist[c] = max(max(max(-ox, ox - (Rg.OX - 1)), max(-oy, oy - (Rg.OY - 1))), 0);
@@ -127,69 +136,95 @@ __device__ __forceinline__ void for_tile(const WaveRegion& Rg, int Y, F fn) {
        (size_t)(Rg.bx0 + wk.row) * Y + Rg.by0 + wk.col);
 }
 
-// Laplacian at shared-memory index i (alpha 1), rows of RY cells.
-__device__ __forceinline__ float lap5s(const float* sm, int i, int RY, const float* w) {
+// ---- shared-memory layout ---------------------------------------------------
+// A region's cells are interleaved, NB floats per cell, so a cell's time levels
+// and K sit at fixed offsets from one base: every access of a step is the cell's
+// base plus a constant (neighbours: +-NB along y, +-NB*RY along x).  Leapfrog
+// keeps two levels per field: step n overwrites u^{n-1}, which only its own cell
+// reads, with u^{n+1}, so the two levels swap roles every step (parity
+// p = s & 1) and the step loop runs two steps per iteration with p a
+// compile-time constant.  The adjoint does the same with mu^{n+2} and keeps two
+// levels of K o mu (its neighbours are read while the next level is written).
+//   forward  (NB 3): 0, 1 levels of u (u^n in 1 - p, u^{n-1} in p), 2 K
+//   adjoint  (NB 5): 0, 1 levels of mu (mu^{n+1} in 1 - p), 2, 3 levels of K o mu
+//                    (K o mu^{n+1} in 3 - p), 4 K
+//   paired   (NB 7): 0, 1 u; 2, 3 mu; 4, 5 K o mu; 6 K
+template <int V>
+using IC = std::integral_constant<int, V>;
+
+// Laplacian (alpha 1) around the interleaved element c: rows rs floats apart,
+// neighbours along y NB floats apart; the reference's term order.
+template <int NB>
+__device__ __forceinline__ float lap5n(const float* c, int rs, const float* w) {
   float acc = 0.0f;
-  acc = add(acc, mul(w[0], sm[i - RY]));
-  acc = add(acc, mul(w[1], sm[i]));
-  acc = add(acc, mul(w[2], sm[i + RY]));
-  acc = add(acc, mul(w[0], sm[i - 1]));
-  acc = add(acc, mul(w[1], sm[i]));
-  acc = add(acc, mul(w[2], sm[i + 1]));
+  acc = add(acc, mul(w[0], c[-rs]));
+  acc = add(acc, mul(w[1], c[0]));
+  acc = add(acc, mul(w[2], c[rs]));
+  acc = add(acc, mul(w[0], c[-NB]));
+  acc = add(acc, mul(w[1], c[0]));
+  acc = add(acc, mul(w[2], c[NB]));
   return acc;
 }
 
-// k forward steps; the three levels are rotated as offsets into the one
-// shared-memory array (om: u^{n-1}, o0: u^n, op: u^{n+1}).
+__device__ __forceinline__ int wave_src_index(const WaveParams& P, const WaveRegion& Rg) {
+  return (P.srcx >= 0 && P.srcx >= Rg.rx0 && P.srcx < Rg.rx0 + Rg.RX && P.srcy >= Rg.ry0 &&
+          P.srcy < Rg.ry0 + Rg.RY)
+             ? (P.srcx - Rg.rx0) * Rg.RY + (P.srcy - Rg.ry0)
+             : -1;
+}
+
+// k forward steps: u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source), written over u^{n-1}.
 template <bool STORE, int MAXC>
-__device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRegion& Rg, float* sm, int& om,
-                                               int& o0, int& op, int ok) {
-  const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
+__device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRegion& Rg, float* sm) {
+  constexpr int NB = 3;
+  const int RY = Rg.RY, rs = NB * RY;
   const WaveRect Rt(P, Rg);
-  const int nt = (int)blockDim.x;
-  const int srci = (P.srcx >= 0 && P.srcx >= rx0 && P.srcx < rx0 + Rg.RX && P.srcy >= ry0 && P.srcy < ry0 + RY)
-                       ? (P.srcx - rx0) * RY + (P.srcy - ry0) : -1;
+  const int srci = wave_src_index(P, Rg);
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, P.Y);
     float kc[MAXC];  // K of the thread's cells (constant over the pass)
 #pragma unroll
-    for (int c = 0; c < MAXC; ++c) kc[c] = C.ri[c] >= 0 ? sm[ok + C.ri[c]] : 0.0f;
-    for (int s = 0; s < P.k; ++s) {
+    for (int c = 0; c < MAXC; ++c) kc[c] = C.ri[c] >= 0 ? sm[NB * C.ri[c] + 2] : 0.0f;
+    auto step = [&](auto PAR, int s) {
+      constexpr int p = decltype(PAR)::value;
       const float sn = (srci >= 0) ? P.src[P.n0 + s] : 0.0f;
       float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
       const int reach = P.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
-        const int i = C.ri[c];
-        if (i < 0 || C.dist[c] > reach) continue;
-        const float lap = lap5s(sm, o0 + i, RY, P.w);
-        float v = sub(mul(2.0f, sm[o0 + i]), sm[om + i]);
+        if (C.dist[c] > reach) continue;  // past the rectangle: dist is out of reach
+        float* pc = sm + NB * C.ri[c];
+        const float lap = lap5n<NB>(pc + (1 - p), rs, P.w);
+        float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
         v = add(v, mul(kc[c], lap));
-        if (i == srci) v = add(v, sn);
-        sm[op + i] = v;
+        if (C.ri[c] == srci) v = add(v, sn);
+        pc[p] = v;
         if (STORE && C.gi[c] >= 0) Ls[C.gi[c]] = lap;
       }
       __syncthreads();
-      const int t = om;
-      om = o0;
-      o0 = op;
-      op = t;
+    };
+    for (int s = 0; s < P.k; s += 2) {
+      step(IC<0>{}, s);
+      if (s + 1 < P.k) step(IC<1>{}, s + 1);
     }
     return;
   }
   // the tile in rectangle coordinates (for the stored Laplacians)
-  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
+  const int nt = (int)blockDim.x;
+  const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
   for (int s = 0; s < P.k; ++s) {
+    const int p = s & 1;
     const float sn = (srci >= 0) ? P.src[P.n0 + s] : 0.0f;
     float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
     RectWalk wk(Rt.W, nt);
     for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
       const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
-      const float lap = lap5s(sm, o0 + i, RY, P.w);
-      float v = sub(mul(2.0f, sm[o0 + i]), sm[om + i]);
-      v = add(v, mul(sm[ok + i], lap));
+      float* pc = sm + NB * i;
+      const float lap = lap5n<NB>(pc + (1 - p), rs, P.w);
+      float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
+      v = add(v, mul(pc[2], lap));
       if (i == srci) v = add(v, sn);
-      sm[op + i] = v;
+      pc[p] = v;
       if (STORE) {
         const int ox = wk.row - tx0, oy = wk.col - ty0;
         if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY)
@@ -197,10 +232,6 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
       }
     }
     __syncthreads();
-    const int t = om;
-    om = o0;
-    o0 = op;
-    op = t;
   }
 }
 
@@ -210,24 +241,23 @@ __global__ void __launch_bounds__(1024) wave_fwd_tb_kernel(const float* __restri
                                                             const float* __restrict__ Kf, float* __restrict__ um_out,
                                                             float* __restrict__ u0_out, const WaveParams P) {
   extern __shared__ __align__(16) float sm[];
+  constexpr int NB = 3;
   const WaveRegion Rg(P, P.k);
-  int om = 0, o0 = P.RC, op = 2 * P.RC;
-  const int ok = 3 * P.RC;
   for_region(Rg, [&](int i, int x, int y) {
     const size_t gi = (size_t)x * P.Y + y;
     const bool in = wave_inside(P, x, y);  // the state is zero outside the node ring
-    cp_async4(sm + om + i, um_in + gi, in);
-    cp_async4(sm + o0 + i, u0_in + gi, in);
-    cp_async4(sm + ok + i, Kf + gi, true);
-    sm[op + i] = 0.0f;
+    cp_async4(sm + NB * i, um_in + gi, in);
+    cp_async4(sm + NB * i + 1, u0_in + gi, in);
+    cp_async4(sm + NB * i + 2, Kf + gi, true);
   });
   cp_async_wait_all();
   __syncthreads();
-  if (P.lst) wave_fwd_steps<true, MAXC>(P, Rg, sm, om, o0, op, ok);
-  else wave_fwd_steps<false, MAXC>(P, Rg, sm, om, o0, op, ok);
+  if (P.lst) wave_fwd_steps<true, MAXC>(P, Rg, sm);
+  else wave_fwd_steps<false, MAXC>(P, Rg, sm);
+  const int nw = (P.k & 1) ? 0 : 1;  // level the last step wrote
   for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
-    um_out[gi] = sm[om + ri];
-    u0_out[gi] = sm[o0 + ri];
+    um_out[gi] = sm[NB * ri + (1 - nw)];
+    u0_out[gi] = sm[NB * ri + nw];
   });
 }
 
@@ -240,24 +270,22 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
                                                             const float* __restrict__ Kf, float* __restrict__ m1_out,
                                                             float* __restrict__ m2_out, const WaveParams P) {
   extern __shared__ __align__(16) float sm[];
+  constexpr int NB = 5;
   const WaveRegion Rg(P, P.k);
-  const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
-  // offsets into sm: mu^{n+2}, mu^{n+1}, mu^n; K o mu^{n+1}, K o mu^n; K; dJ/dK of the tile
-  int o2 = 0, o1 = P.RC, o0 = 2 * P.RC, k1 = 3 * P.RC, k0 = 4 * P.RC;
-  const int okk = 5 * P.RC, oga = 6 * P.RC;
+  const int RY = Rg.RY, rs = NB * RY;
+  const int oga = NB * P.RC;  // dJ/dK of the tile (MAXC = 0)
   for_region(Rg, [&](int i, int x, int y) {
     const size_t gi = (size_t)x * P.Y + y;
     const bool in = wave_inside(P, x, y);
-    cp_async4(sm + o2 + i, m2_in + gi, in);
-    cp_async4(sm + o1 + i, m1_in + gi, in);
-    cp_async4(sm + okk + i, Kf + gi, true);
-    sm[o0 + i] = 0.0f;
-    sm[k0 + i] = 0.0f;
+    cp_async4(sm + NB * i, m2_in + gi, in);      // mu^{n+2}
+    cp_async4(sm + NB * i + 1, m1_in + gi, in);  // mu^{n+1}
+    cp_async4(sm + NB * i + 4, Kf + gi, true);
+    sm[NB * i + 2] = 0.0f;
   });
   if (MAXC == 0) for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, P.gK + gi, true); });
   cp_async_wait_all();
   // K o mu^{n+1} of the cells this thread copied (its own copies are complete)
-  for_region(Rg, [&](int i, int x, int y) { sm[k1 + i] = mul(sm[okk + i], sm[o1 + i]); });
+  for_region(Rg, [&](int i, int x, int y) { sm[NB * i + 3] = mul(sm[NB * i + 4], sm[NB * i + 1]); });
   __syncthreads();
   const WaveRect Rt(P, Rg);
   if constexpr (MAXC > 0) {
@@ -268,9 +296,10 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
     for (int c = 0; c < MAXC; ++c) {
       ga[c] = C.gi[c] >= 0 ? P.gK[C.gi[c]] : 0.0f;
       lnext[c] = C.gi[c] >= 0 ? __ldg(L0 + C.gi[c]) : 0.0f;
-      kc[c] = C.ri[c] >= 0 ? sm[okk + C.ri[c]] : 0.0f;  // K of the thread's cells
+      kc[c] = C.ri[c] >= 0 ? sm[NB * C.ri[c] + 4] : 0.0f;  // K of the thread's cells
     }
-    for (int s = 0; s < P.k; ++s) {
+    auto step = [&](auto PAR, int s) {
+      constexpr int p = decltype(PAR)::value;
       float ln[MAXC];
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) ln[c] = lnext[c];
@@ -283,67 +312,57 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
       const int reach = P.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
-        const int i = C.ri[c];
-        if (i < 0 || C.dist[c] > reach) continue;
-        const float m1 = sm[o1 + i];
+        if (C.dist[c] > reach) continue;
+        float* pc = sm + NB * C.ri[c];
+        const float m1 = pc[1 - p];
         if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
-        const float acc = lap5s(sm, k1 + i, RY, P.w);
-        const float v = add(sub(mul(2.0f, m1), sm[o2 + i]), acc);
-        sm[o0 + i] = v;
-        sm[k0 + i] = mul(kc[c], v);
+        // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+        const float acc = lap5n<NB>(pc + (3 - p), rs, P.w);
+        const float v = add(sub(mul(2.0f, m1), pc[p]), acc);
+        pc[p] = v;
+        pc[2 + p] = mul(kc[c], v);
       }
       __syncthreads();
-      const int t = o2;
-      o2 = o1;
-      o1 = o0;
-      o0 = t;
-      const int u = k1;
-      k1 = k0;
-      k0 = u;
+    };
+    for (int s = 0; s < P.k; s += 2) {
+      step(IC<0>{}, s);
+      if (s + 1 < P.k) step(IC<1>{}, s + 1);
     }
 #pragma unroll
     for (int c = 0; c < MAXC; ++c)
       if (C.gi[c] >= 0) P.gK[C.gi[c]] = ga[c];
-    for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
-      m1_out[gi] = sm[o1 + ri];
-      m2_out[gi] = sm[o2 + ri];
-    });
-    return;
-  }
-  const int nt = (int)blockDim.x;
-  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
-  for (int s = 0; s < P.k; ++s) {
-    const float* Ln = P.lsts + (size_t)(P.ntop - s) * P.cells;
-    RectWalk wk(Rt.W, nt);
-    for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
-      const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
-      const float m1 = sm[o1 + i];
-      {  // gradient term of step n on the tile: dJ/dK += mu^{n+1} o L(u^n)
-        const int ox = wk.row - tx0, oy = wk.col - ty0;
-        if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) {
-          const int t = oga + ox * Rg.OY + oy;
-          sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * P.Y + Rg.by0 + oy)));
+  } else {
+    const int nt = (int)blockDim.x;
+    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
+    for (int s = 0; s < P.k; ++s) {
+      const int p = s & 1;
+      const float* Ln = P.lsts + (size_t)(P.ntop - s) * P.cells;
+      RectWalk wk(Rt.W, nt);
+      for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
+        const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
+        float* pc = sm + NB * i;
+        const float m1 = pc[1 - p];
+        {  // gradient term of step n on the tile: dJ/dK += mu^{n+1} o L(u^n)
+          const int ox = wk.row - tx0, oy = wk.col - ty0;
+          if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) {
+            const int t = oga + ox * Rg.OY + oy;
+            sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * P.Y + Rg.by0 + oy)));
+          }
         }
+        // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+        const float acc = lap5n<NB>(pc + (3 - p), rs, P.w);
+        const float v = add(sub(mul(2.0f, m1), pc[p]), acc);
+        pc[p] = v;
+        pc[2 + p] = mul(pc[4], v);
       }
-      // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
-      const float acc = lap5s(sm, k1 + i, RY, P.w);
-      const float v = add(sub(mul(2.0f, m1), sm[o2 + i]), acc);
-      sm[o0 + i] = v;
-      sm[k0 + i] = mul(sm[okk + i], v);
+      __syncthreads();
     }
-    __syncthreads();
-    const int t = o2;
-    o2 = o1;
-    o1 = o0;
-    o0 = t;
-    const int u = k1;
-    k1 = k0;
-    k0 = u;
+    for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) { P.gK[gi] = sm[oga + t]; });
   }
+  const int nw = (P.k & 1) ? 0 : 1;  // level the last step wrote
   for_tile(Rg, P.Y, [&](int t, int ri, size_t gi) {
-    m1_out[gi] = sm[o1 + ri];
-    m2_out[gi] = sm[o2 + ri];
-    P.gK[gi] = sm[oga + t];
+    m1_out[gi] = sm[NB * ri + nw];
+    m2_out[gi] = sm[NB * ri + (1 - nw)];
   });
 }
 
@@ -353,10 +372,9 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
 // up to k adjoint steps of another segment (as wave_adj_tb_kernel).  The two
 // are independent, so each warp interleaves two dependency chains and a step
 // of both costs one barrier.  Arithmetic and per-cell operation order are
-// those of the two kernels above.  Shared memory (offsets of RC cells): forward
-// levels 0-2, adjoint levels 3-5, K o mu 6-7, K 8, then the gradient tile.
-// MAXC as in wave_adj_tb_kernel (the forward's stored Laplacians use the same
-// tile indices).
+// those of the two kernels above.  Shared memory: the NB = 7 interleaved
+// region, then the gradient tile (MAXC = 0).  MAXC as in wave_adj_tb_kernel
+// (the forward's stored Laplacians use the same tile indices).
 template <int MAXC>
 __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restrict__ um_in,
                                                              const float* __restrict__ u0_in,
@@ -367,38 +385,34 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
                                                              const float* __restrict__ Kf, const WaveParams Pf,
                                                              const WaveParams Pa) {
   extern __shared__ __align__(16) float sm[];
+  constexpr int NB = 7;
   const int H = max(Pf.k, Pa.k);
   const WaveRegion Rg(Pa, H);  // Pf and Pa share the grid, tile and region capacity
-  const int RY = Rg.RY, rx0 = Rg.rx0, ry0 = Rg.ry0;
-  const int RC = Pa.RC;
-  int fm = 0, f0 = RC, fp = 2 * RC;
-  int a2 = 3 * RC, a1 = 4 * RC, a0 = 5 * RC, k1 = 6 * RC, k0 = 7 * RC;
-  const int okk = 8 * RC, oga = 9 * RC;
+  const int RY = Rg.RY, rs = NB * RY;
+  const int oga = NB * Pa.RC;
   const bool fwd = Pf.k > 0, adj = Pa.k > 0;
   for_region(Rg, [&](int i, int x, int y) {
     const size_t gi = (size_t)x * Pa.Y + y;
     const bool in = wave_inside(Pa, x, y);  // the states are zero outside the node ring
-    cp_async4(sm + okk + i, Kf + gi, true);
+    float* pc = sm + NB * i;
+    cp_async4(pc + 6, Kf + gi, true);
     if (fwd) {
-      cp_async4(sm + fm + i, um_in + gi, in);
-      cp_async4(sm + f0 + i, u0_in + gi, in);
-      sm[fp + i] = 0.0f;
+      cp_async4(pc, um_in + gi, in);
+      cp_async4(pc + 1, u0_in + gi, in);
     }
     if (adj) {
-      cp_async4(sm + a2 + i, m2_in + gi, in);
-      cp_async4(sm + a1 + i, m1_in + gi, in);
-      sm[a0 + i] = 0.0f;
-      sm[k0 + i] = 0.0f;
+      cp_async4(pc + 2, m2_in + gi, in);
+      cp_async4(pc + 3, m1_in + gi, in);
+      pc[4] = 0.0f;
     }
   });
   if (adj && MAXC == 0)
     for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, Pa.gK + gi, true); });
   cp_async_wait_all();
-  if (adj) for_region(Rg, [&](int i, int x, int y) { sm[k1 + i] = mul(sm[okk + i], sm[a1 + i]); });
+  if (adj) for_region(Rg, [&](int i, int x, int y) { sm[NB * i + 5] = mul(sm[NB * i + 6], sm[NB * i + 3]); });
   __syncthreads();
   const WaveRect Rt(Pa, Rg);
-  const int srci = (Pf.srcx >= 0 && Pf.srcx >= rx0 && Pf.srcx < rx0 + Rg.RX && Pf.srcy >= ry0 && Pf.srcy < ry0 + RY)
-                       ? (Pf.srcx - rx0) * RY + (Pf.srcy - ry0) : -1;
+  const int srci = wave_src_index(Pf, Rg);
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, Pa.Y);
     float ga[MAXC], lnext[MAXC], kc[MAXC];
@@ -406,14 +420,15 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
     for (int c = 0; c < MAXC; ++c) {
       ga[c] = 0.0f;
       lnext[c] = 0.0f;
-      kc[c] = C.ri[c] >= 0 ? sm[okk + C.ri[c]] : 0.0f;  // K of the thread's cells, for both chains
+      kc[c] = C.ri[c] >= 0 ? sm[NB * C.ri[c] + 6] : 0.0f;  // K of the thread's cells, for both chains
       if (adj && C.gi[c] >= 0) {
         ga[c] = Pa.gK[C.gi[c]];
         lnext[c] = __ldg(Pa.lsts + (size_t)Pa.ntop * Pa.cells + C.gi[c]);
       }
     }
-    for (int s = 0; s < H; ++s) {
-      const bool fs = s < Pf.k, as = s < Pa.k;
+    auto step = [&](auto PAR, int s) {
+      constexpr int p = decltype(PAR)::value;
+      const bool fs = s < Pf.k;
       const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
       float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
       float ln[MAXC];
@@ -425,122 +440,90 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
         for (int c = 0; c < MAXC; ++c)
           if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
       }
+      // a chain past its last step has a negative reach (dist >= 0)
       const int freach = Pf.k - 1 - s, areach = Pa.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
-        const int i = C.ri[c];
-        if (i < 0) continue;
-        if (fs && C.dist[c] <= freach) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
-          const float lap = lap5s(sm, f0 + i, RY, Pf.w);
-          float v = sub(mul(2.0f, sm[f0 + i]), sm[fm + i]);
+        float* pc = sm + NB * C.ri[c];
+        if (C.dist[c] <= freach) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+          const float lap = lap5n<NB>(pc + (1 - p), rs, Pf.w);
+          float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
           v = add(v, mul(kc[c], lap));
-          if (i == srci) v = add(v, sn);
-          sm[fp + i] = v;
+          if (C.ri[c] == srci) v = add(v, sn);
+          pc[p] = v;
           if (C.gi[c] >= 0) Ls[C.gi[c]] = lap;
         }
-        if (as && C.dist[c] <= areach) {
-          const float m1 = sm[a1 + i];
+        if (C.dist[c] <= areach) {
+          const float m1 = pc[3 - p];
           if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
           // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
-          const float acc = lap5s(sm, k1 + i, RY, Pa.w);
-          const float v = add(sub(mul(2.0f, m1), sm[a2 + i]), acc);
-          sm[a0 + i] = v;
-          sm[k0 + i] = mul(kc[c], v);
+          const float acc = lap5n<NB>(pc + (5 - p), rs, Pa.w);
+          const float v = add(sub(mul(2.0f, m1), pc[2 + p]), acc);
+          pc[2 + p] = v;
+          pc[4 + p] = mul(kc[c], v);
         }
       }
       __syncthreads();
-      if (fs) {
-        const int t = fm;
-        fm = f0;
-        f0 = fp;
-        fp = t;
-      }
-      if (as) {
-        int t = a2;
-        a2 = a1;
-        a1 = a0;
-        a0 = t;
-        t = k1;
-        k1 = k0;
-        k0 = t;
-      }
+    };
+    for (int s = 0; s < H; s += 2) {
+      step(IC<0>{}, s);
+      if (s + 1 < H) step(IC<1>{}, s + 1);
     }
     if (adj) {
 #pragma unroll
       for (int c = 0; c < MAXC; ++c)
         if (C.gi[c] >= 0) Pa.gK[C.gi[c]] = ga[c];
     }
-    for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) {
-      if (fwd) {
-        um_out[gi] = sm[fm + ri];
-        u0_out[gi] = sm[f0 + ri];
-      }
-      if (adj) {
-        m1_out[gi] = sm[a1 + ri];
-        m2_out[gi] = sm[a2 + ri];
-      }
-    });
-    return;
-  }
-  const int nt = (int)blockDim.x;
-  const int tx0 = Rg.bx0 - rx0 - Rt.cx0, ty0 = Rg.by0 - ry0 - Rt.cy0;
-  for (int s = 0; s < H; ++s) {
-    const bool fs = s < Pf.k, as = s < Pa.k;
-    const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
-    float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
-    const float* Ln = as ? Pa.lsts + (size_t)(Pa.ntop - s) * Pa.cells : nullptr;
-    RectWalk wk(Rt.W, nt);
-    for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
-      const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
-      const int ox = wk.row - tx0, oy = wk.col - ty0;
-      const bool tile = ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY;
-      if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
-        const float lap = lap5s(sm, f0 + i, RY, Pf.w);
-        float v = sub(mul(2.0f, sm[f0 + i]), sm[fm + i]);
-        v = add(v, mul(sm[okk + i], lap));
-        if (i == srci) v = add(v, sn);
-        sm[fp + i] = v;
-        if (tile) Ls[(size_t)(Rg.bx0 + ox) * Pf.Y + Rg.by0 + oy] = lap;
-      }
-      if (as) {
-        const float m1 = sm[a1 + i];
-        if (tile) {  // dJ/dK += mu^{n+1} o L(u^n)
-          const int t = oga + ox * Rg.OY + oy;
-          sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * Pa.Y + Rg.by0 + oy)));
+  } else {
+    const int nt = (int)blockDim.x;
+    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
+    for (int s = 0; s < H; ++s) {
+      const int p = s & 1;
+      const bool fs = s < Pf.k, as = s < Pa.k;
+      const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
+      float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
+      const float* Ln = as ? Pa.lsts + (size_t)(Pa.ntop - s) * Pa.cells : nullptr;
+      RectWalk wk(Rt.W, nt);
+      for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
+        const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
+        float* pc = sm + NB * i;
+        const int ox = wk.row - tx0, oy = wk.col - ty0;
+        const bool tile = ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY;
+        if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+          const float lap = lap5n<NB>(pc + (1 - p), rs, Pf.w);
+          float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
+          v = add(v, mul(pc[6], lap));
+          if (i == srci) v = add(v, sn);
+          pc[p] = v;
+          if (tile) Ls[(size_t)(Rg.bx0 + ox) * Pf.Y + Rg.by0 + oy] = lap;
         }
-        // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
-        const float acc = lap5s(sm, k1 + i, RY, Pa.w);
-        const float v = add(sub(mul(2.0f, m1), sm[a2 + i]), acc);
-        sm[a0 + i] = v;
-        sm[k0 + i] = mul(sm[okk + i], v);
+        if (as) {
+          const float m1 = pc[3 - p];
+          if (tile) {  // dJ/dK += mu^{n+1} o L(u^n)
+            const int t = oga + ox * Rg.OY + oy;
+            sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * Pa.Y + Rg.by0 + oy)));
+          }
+          // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+          const float acc = lap5n<NB>(pc + (5 - p), rs, Pa.w);
+          const float v = add(sub(mul(2.0f, m1), pc[2 + p]), acc);
+          pc[2 + p] = v;
+          pc[4 + p] = mul(pc[6], v);
+        }
       }
+      __syncthreads();
     }
-    __syncthreads();
-    if (fs) {
-      const int t = fm;
-      fm = f0;
-      f0 = fp;
-      fp = t;
-    }
-    if (as) {
-      int t = a2;
-      a2 = a1;
-      a1 = a0;
-      a0 = t;
-      t = k1;
-      k1 = k0;
-      k0 = t;
-    }
+    if (adj) for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { Pa.gK[gi] = sm[oga + t]; });
   }
+  const int fw = (Pf.k & 1) ? 0 : 1, aw = (Pa.k & 1) ? 0 : 1;  // levels the last steps wrote
   for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) {
+    const float* pc = sm + NB * ri;
     if (fwd) {
-      um_out[gi] = sm[fm + ri];
-      u0_out[gi] = sm[f0 + ri];
+      um_out[gi] = pc[1 - fw];
+      u0_out[gi] = pc[fw];
     }
     if (adj) {
-      m1_out[gi] = sm[a1 + ri];
-      m2_out[gi] = sm[a2 + ri];
-      Pa.gK[gi] = sm[oga + t];
+      m1_out[gi] = pc[2 + aw];
+      m2_out[gi] = pc[3 - aw];
     }
   });
 }
