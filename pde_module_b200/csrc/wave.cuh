@@ -96,23 +96,29 @@ struct WaveRect {
 template <int MAXC>
 struct WaveCells {
   int ri[MAXC];    // region index; -1 for an idle slot
-  int gi[MAXC];    // array index of a tile cell; -1 for the other cells
+  int gi[MAXC];    // array index of a tile cell; 0 (a valid address) for the other cells
   int dist[MAXC];  // distance from the tile; 1 << 20 for an idle slot
+  unsigned tile;   // bit c: slot c holds a tile cell
+  __device__ bool is_tile(int c) const { return (tile >> c) & 1u; }
   __device__ WaveCells(const WaveRect& Rt, const WaveRegion& Rg, int Y) {
     const int nt = (int)blockDim.x;
     // tile origin: rows relative to the rectangle, columns relative to the region
     const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0;
     const int n = Rt.NR * Rg.RY;
     RectWalk wk(Rg.RY, nt);
+    tile = 0;
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
       ri[c] = -1;
-      gi[c] = -1;
+      gi[c] = 0;
       dist[c] = 1 << 20;
       if ((int)threadIdx.x + c * nt < n && wk.col >= Rt.cy0 && wk.col < Rt.cy0 + Rt.W) {
         ri[c] = (Rt.cx0 + wk.row) * Rg.RY + wk.col;
         const int ox = wk.row - tx0, oy = wk.col - ty0;
-        if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) gi[c] = (Rg.bx0 + ox) * Y + Rg.by0 + oy;
+        if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) {
+          gi[c] = (Rg.bx0 + ox) * Y + Rg.by0 + oy;
+          tile |= 1u << c;
+        }
         dist[c] = max(max(max(-ox, ox - (Rg.OX - 1)), max(-oy, oy - (Rg.OY - 1))), 0);
       }
       wk.next();
@@ -151,6 +157,14 @@ __device__ __forceinline__ void for_tile(const WaveRegion& Rg, int Y, F fn) {
 //   paired   (NB 7): 0, 1 u; 2, 3 mu; 4, 5 K o mu; 6 K
 template <int V>
 using IC = std::integral_constant<int, V>;
+
+// st.global under a predicate, without a branch around it
+__device__ __forceinline__ void st_global_if(float* p, float v, bool on) {
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.b32 q, %2, 0;\n @q st.global.f32 [%0], %1;\n}\n" ::"l"(p), "f"(v),
+      "r"((int)on)
+      : "memory");
+}
 
 // Laplacian (alpha 1) around the interleaved element c: rows rs floats apart,
 // neighbours along y NB floats apart; the reference's term order.
@@ -199,7 +213,7 @@ __device__ __forceinline__ void wave_fwd_steps(const WaveParams& P, const WaveRe
         v = add(v, mul(kc[c], lap));
         if (C.ri[c] == srci) v = add(v, sn);
         pc[p] = v;
-        if (STORE && C.gi[c] >= 0) Ls[C.gi[c]] = lap;
+        if (STORE) st_global_if(Ls + C.gi[c], lap, C.is_tile(c));
       }
       __syncthreads();
     };
@@ -290,37 +304,36 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
   const WaveRect Rt(P, Rg);
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, P.Y);
-    float ga[MAXC], lnext[MAXC], kc[MAXC];
+    // lv: L(u^n) of the step at the thread's cells, the next step's issued before
+    // each barrier; the other cells load from index 0 and their gradient sums go
+    // unused (no per-cell branches)
+    float ga[MAXC], lv[MAXC], kc[MAXC];
     const float* L0 = P.lsts + (size_t)P.ntop * P.cells;
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
-      ga[c] = C.gi[c] >= 0 ? P.gK[C.gi[c]] : 0.0f;
-      lnext[c] = C.gi[c] >= 0 ? __ldg(L0 + C.gi[c]) : 0.0f;
+      ga[c] = C.is_tile(c) ? P.gK[C.gi[c]] : 0.0f;
+      lv[c] = __ldg(L0 + C.gi[c]);
       kc[c] = C.ri[c] >= 0 ? sm[NB * C.ri[c] + 4] : 0.0f;  // K of the thread's cells
     }
     auto step = [&](auto PAR, int s) {
       constexpr int p = decltype(PAR)::value;
-      float ln[MAXC];
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) ln[c] = lnext[c];
-      if (s + 1 < P.k) {
-        const float* L1 = P.lsts + (size_t)(P.ntop - s - 1) * P.cells;
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
-      }
       const int reach = P.k - 1 - s;
 #pragma unroll
       for (int c = 0; c < MAXC; ++c) {
         if (C.dist[c] > reach) continue;
         float* pc = sm + NB * C.ri[c];
         const float m1 = pc[1 - p];
-        if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
+        ga[c] = add(ga[c], mul(m1, lv[c]));  // dJ/dK += mu^{n+1} o L(u^n) (kept for tile cells)
         // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
         const float acc = lap5n<NB>(pc + (3 - p), rs, P.w);
         const float v = add(sub(mul(2.0f, m1), pc[p]), acc);
         pc[p] = v;
         pc[2 + p] = mul(kc[c], v);
+      }
+      if (s + 1 < P.k) {
+        const float* L1 = P.lsts + (size_t)(P.ntop - s - 1) * P.cells;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c) lv[c] = __ldg(L1 + C.gi[c]);
       }
       __syncthreads();
     };
@@ -330,7 +343,7 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
     }
 #pragma unroll
     for (int c = 0; c < MAXC; ++c)
-      if (C.gi[c] >= 0) P.gK[C.gi[c]] = ga[c];
+      if (C.is_tile(c)) P.gK[C.gi[c]] = ga[c];
   } else {
     const int nt = (int)blockDim.x;
     const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
@@ -415,15 +428,17 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
   const int srci = wave_src_index(Pf, Rg);
   if constexpr (MAXC > 0) {
     const WaveCells<MAXC> C(Rt, Rg, Pa.Y);
-    float ga[MAXC], lnext[MAXC], kc[MAXC];
+    // lv as in wave_adj_tb_kernel; the forward's Laplacians are stored with a
+    // predicated store (tile cells only)
+    float ga[MAXC], lv[MAXC], kc[MAXC];
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
       ga[c] = 0.0f;
-      lnext[c] = 0.0f;
+      lv[c] = 0.0f;
       kc[c] = C.ri[c] >= 0 ? sm[NB * C.ri[c] + 6] : 0.0f;  // K of the thread's cells, for both chains
-      if (adj && C.gi[c] >= 0) {
-        ga[c] = Pa.gK[C.gi[c]];
-        lnext[c] = __ldg(Pa.lsts + (size_t)Pa.ntop * Pa.cells + C.gi[c]);
+      if (adj) {
+        if (C.is_tile(c)) ga[c] = Pa.gK[C.gi[c]];
+        lv[c] = __ldg(Pa.lsts + (size_t)Pa.ntop * Pa.cells + C.gi[c]);
       }
     }
     auto step = [&](auto PAR, int s) {
@@ -431,15 +446,6 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
       const bool fs = s < Pf.k;
       const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
       float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
-      float ln[MAXC];
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) ln[c] = lnext[c];
-      if (s + 1 < Pa.k) {
-        const float* L1 = Pa.lsts + (size_t)(Pa.ntop - s - 1) * Pa.cells;
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c)
-          if (C.gi[c] >= 0) lnext[c] = __ldg(L1 + C.gi[c]);
-      }
       // a chain past its last step has a negative reach (dist >= 0)
       const int freach = Pf.k - 1 - s, areach = Pa.k - 1 - s;
 #pragma unroll
@@ -451,17 +457,22 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
           v = add(v, mul(kc[c], lap));
           if (C.ri[c] == srci) v = add(v, sn);
           pc[p] = v;
-          if (C.gi[c] >= 0) Ls[C.gi[c]] = lap;
+          st_global_if(Ls + C.gi[c], lap, C.is_tile(c));
         }
         if (C.dist[c] <= areach) {
           const float m1 = pc[3 - p];
-          if (C.gi[c] >= 0) ga[c] = add(ga[c], mul(m1, ln[c]));  // dJ/dK += mu^{n+1} o L(u^n)
+          ga[c] = add(ga[c], mul(m1, lv[c]));  // dJ/dK += mu^{n+1} o L(u^n) (kept for tile cells)
           // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
           const float acc = lap5n<NB>(pc + (5 - p), rs, Pa.w);
           const float v = add(sub(mul(2.0f, m1), pc[2 + p]), acc);
           pc[2 + p] = v;
           pc[4 + p] = mul(kc[c], v);
         }
+      }
+      if (s + 1 < Pa.k) {  // the next step's L(u^n), in flight across the barrier
+        const float* L1 = Pa.lsts + (size_t)(Pa.ntop - s - 1) * Pa.cells;
+#pragma unroll
+        for (int c = 0; c < MAXC; ++c) lv[c] = __ldg(L1 + C.gi[c]);
       }
       __syncthreads();
     };
@@ -472,7 +483,7 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
     if (adj) {
 #pragma unroll
       for (int c = 0; c < MAXC; ++c)
-        if (C.gi[c] >= 0) Pa.gK[C.gi[c]] = ga[c];
+        if (C.is_tile(c)) Pa.gK[C.gi[c]] = ga[c];
     }
   } else {
     const int nt = (int)blockDim.x;
