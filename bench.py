@@ -618,7 +618,7 @@ def run_ldc(steps: int = 2000, n: int = 1024):
     import pde_module_b200._lib as L
     tune = {}
     for tile in ((0, 0, 0), (32, 64, 0), (64, 64, 0), (64, 64, 512), (64, 64, 1024), (48, 96, 0), (48, 96, 512),
-                 (32, 128, 0), (32, 128, 512)):
+                 (32, 128, 0), (32, 128, 512), (44, 88, 512), (64, 128, 1024), (88, 88, 1024)):
         L.check(L.lib().pde_set_launch_2d(*tile), "pde_set_launch_2d")
         for kk in (5, 8, 10, 16):
             tune[(tile, kk)] = timed_rollout(kk, 40)

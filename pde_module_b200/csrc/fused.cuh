@@ -153,7 +153,9 @@ __device__ __forceinline__ float step_time(double t0, double tstep, int n) {
 
 // Boundary fill of the smem region (array rectangle [rx0,rx0+RX) x [ry0,ry0+RY)),
 // in place: ghosts first (they read pre-boundary interior values), then nodes.
-template <int N>
+// S: floats per region cell (N for a dense field; more when the field's values
+// are interleaved with other data, A pointing at the field's first value).
+template <int N, int S = N>
 __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, const PdeBCRules& Rl, int rx0, int RX,
                                                int ry0, int RY, float dx32) {
   const int g = P.g, X = P.X, Y = P.Y;
@@ -192,8 +194,8 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
     for (int v = 0; v < N; ++v) {
       const int gi = Rl.ghost_group[K][ax][v];
       if (gi < 0) continue;
-      const float a = A[((qx - rx0) * RY + (qy - ry0)) * N + v];
-      A[((gx - rx0) * RY + (gy - ry0)) * N + v] = ghost_value(Rl, gi, inc, a, dx32);
+      const float a = A[((qx - rx0) * RY + (qy - ry0)) * S + v];
+      A[((gx - rx0) * RY + (gy - ry0)) * S + v] = ghost_value(Rl, gi, inc, a, dx32);
     }
   }
   __syncthreads();
@@ -218,7 +220,7 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
     const float val = Rl.group[gi].value;
 #pragma unroll
     for (int v = 0; v < N; ++v)
-      if ((m >> v) & 1u) A[((x - rx0) * RY + (y - ry0)) * N + v] = val;
+      if ((m >> v) & 1u) A[((x - rx0) * RY + (y - ry0)) * S + v] = val;
   }
   __syncthreads();
 }

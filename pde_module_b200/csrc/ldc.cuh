@@ -11,6 +11,8 @@
 //   p    <- 0.25 * (pW + pE + pS + pN - dx^2 * rhs)      (Jacobi, p_bc = BC_p(p)), 50 sweeps
 //   u    = BC_u(u*) + dt * (-Grad(BC_p(p)))              (projection)
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "fused.cuh"
 
@@ -257,6 +259,123 @@ __global__ void __launch_bounds__(1024) jacobi2d_tb_kernel(const float* __restri
     const int ri = (x - rx0) * RY + (y - ry0);
     const bool st = x >= g && x < P.X - g && y >= g && y < P.Y - g;
     pout[(size_t)x * P.Y + y] = st ? A[ri] : B[ri];  // (equal when k = 0: both hold the loaded values)
+  }
+  if (P.last && resid) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+    __shared__ float wsum[32];
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float b = 0.0f;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b += wsum[w];
+      atomicAdd(resid, b);
+    }
+  }
+}
+
+// The same passes with register cell lists (as the wave kernels): the region's
+// cells interleave the two levels and the right-hand side (3 floats per cell, an
+// odd stride: no bank conflicts), each thread's stencil cells are fixed for the
+// pass (slots q = threadIdx.x + c * blockDim.x over the stencil rectangle's rows
+// at full region width, the columns outside the rectangle idle), with their
+// region index and distance from the tile (one packed word: index in the low 16
+// bits, regions hold fewer than 2^16 cells) and h^2 rhs in registers (h^2 rhs is
+// the same product every sweep).  Sweep s reads level s & 1 and writes the other;
+// two sweeps per loop iteration make the levels compile-time offsets.  Same
+// arithmetic and order per cell as jacobi2d_tb_kernel; needs the rectangle's
+// rows x RY <= MAXC * blockDim.x.
+template <int MAXC>
+__global__ void __launch_bounds__(1024) jacobi2d_cells_kernel(const float* __restrict__ pin,
+                                                              float* __restrict__ pout,
+                                                              const float* __restrict__ rhs,
+                                                              float* __restrict__ resid, const J2Params P,
+                                                              const PdeBCRules Rp) {
+  extern __shared__ __align__(16) float sm[];
+  constexpr int NB = 3;  // per region cell: level 0, level 1, rhs
+  const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
+  const int bx0 = P.own_lo + tx * P.TBX, by0 = ty * P.TBY;
+  const int H = P.k + 1;
+  const int rx0 = max(bx0 - H, P.held_lo), rx1 = min(bx0 + P.TBX + H, P.held_hi);
+  const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
+  const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
+  const int nt = (int)blockDim.x;
+  {
+    RectWalk wk(RY, nt);
+    for (int i = threadIdx.x; i < RC; i += nt, wk.next()) {
+      const size_t gi = (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col;
+      cp_async4(sm + NB * i, pin + gi, true);
+      cp_async4(sm + NB * i + 1, pin + gi, true);
+      cp_async4(sm + NB * i + 2, rhs + gi, true);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  H2Params HP;
+  HP.X = P.X; HP.Y = P.Y; HP.g = P.g; HP.N = 1;
+  const int g = P.g;
+  // stencil rectangle: cells of [g, n-g) whose four neighbours are inside the region
+  const int sx0 = max(g, rx0 + 1) - rx0, sx1 = min(P.X - g, rx0 + RX - 1) - rx0;
+  const int sy0 = max(g, ry0 + 1) - ry0, sy1 = min(P.Y - g, ry0 + RY - 1) - ry0;
+  const int tw = min(bx0 + P.TBX, P.own_hi) - bx0, th = min(by0 + P.TBY, P.Y) - by0;
+  const int tlx = bx0 - rx0, tly = by0 - ry0;  // the tile's origin in the region
+  int key[MAXC];  // region index | distance from the tile << 16; idle slots: INT_MAX
+  float hr[MAXC];
+  unsigned tile = 0;  // bit c: slot c holds a tile cell (residual)
+  {
+    const int n = max(sx1 - sx0, 0) * RY;
+    RectWalk wk(RY, nt);
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      key[c] = 0x7fffffff;
+      hr[c] = 0.0f;
+      if ((int)threadIdx.x + c * nt < n && wk.col >= sy0 && wk.col < sy1) {
+        const int lx = sx0 + wk.row, ly = wk.col;
+        const int r = lx * RY + ly;
+        const int ox = lx - tlx, oy = ly - tly;
+        const int d = max(max(max(-ox, ox - (tw - 1)), max(-oy, oy - (th - 1))), 0);
+        key[c] = r | (d << 16);
+        if (ox >= 0 && ox < tw && oy >= 0 && oy < th) tile |= 1u << c;
+        hr[c] = mul(P.h2, sm[NB * r + 2]);
+      }
+      wk.next();
+    }
+  }
+  const int rs = NB * RY;
+  float sq = 0.0f;
+  // Sweep s only has to update the stencil cells within (k - 1 - s) + 1 of the
+  // tile (the boundary fills read inward): those with dist <= k - s.
+  auto sweep = [&](auto PAR, int s) {
+    constexpr int p = decltype(PAR)::value;  // reads level p, writes level 1 - p
+    bc_fill_region<1, NB>(sm + p, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);
+    const bool acc_res = P.last && s == P.k - 1;
+    const int lim = (P.k - s + 1) << 16;  // dist <= k - s  <=>  key < lim
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      if (key[c] >= lim) continue;
+      float* pc = sm + NB * (key[c] & 0xffff);
+      const float sum = add(add(add(pc[p - rs], pc[p + rs]), pc[p - NB]), pc[p + NB]);
+      const float res = mul(0.25f, sub(sum, hr[c]));
+      if (acc_res && ((tile >> c) & 1u)) {
+        const float d = res - pc[p];
+        sq = fmaf(d, d, sq);
+      }
+      pc[1 - p] = res;
+    }
+    __syncthreads();
+  };
+  for (int s = 0; s < P.k; s += 2) {
+    sweep(std::integral_constant<int, 0>{}, s);
+    if (s + 1 < P.k) sweep(std::integral_constant<int, 1>{}, s + 1);
+  }
+  // output: stencil cells from the newest level, the others as last filled
+  const int nw = P.k & 1;  // the level the last sweep wrote
+  RectWalk wo(th, nt);
+  for (int i = threadIdx.x; i < tw * th; i += nt, wo.next()) {
+    const int x = bx0 + wo.row, y = by0 + wo.col;
+    const int r = (x - rx0) * RY + (y - ry0);
+    const bool st = x >= g && x < P.X - g && y >= g && y < P.Y - g;
+    pout[(size_t)x * P.Y + y] = sm[NB * r + (st ? nw : 1 - nw)];
   }
   if (P.last && resid) {
 #pragma unroll

@@ -1040,21 +1040,67 @@ int ldc_setup(const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* 
 
 // Jacobi launch geometry for k sweeps per pass over owned rows [own_lo, own_hi)
 // of arrays holding rows [held_lo, held_hi) of a domain of G.n[0] rows.
+struct JacobiLaunch {
+  int tiles, threads, cpt;  // cpt: register cells per thread (0: the flat-walk kernel)
+  size_t smem;
+};
+
 int jacobi_setup(const Geo& G, float h2, int k, int own_lo, int own_hi, int held_lo, int held_hi, J2Params* JP,
-                 int* tiles, size_t* smem) {
+                 JacobiLaunch* L) {
   JP->X = (int)G.n[0]; JP->Y = (int)G.n[1]; JP->g = G.g;
   JP->own_lo = own_lo; JP->own_hi = own_hi; JP->held_lo = held_lo; JP->held_hi = held_hi;
-  pick_tile_2d(JP->X, JP->Y, &JP->TBX, &JP->TBY);
+  bool placed = false;
+  if (g_tile2d[0] == 0 && g_threads2d == 0) {
+    // automatic shape on grids that fill the SMs: one near-square tile per SM,
+    // 1024 threads (the register cell-list kernel, at most 12 cells per thread)
+    const int rows = own_hi - own_lo, sms = (int)sm_count();
+    int nx = (int)lround(sqrt((double)sms * rows / JP->Y));
+    nx = nx < 1 ? 1 : (nx > sms ? sms : nx);
+    const int ny = sms / nx > 0 ? sms / nx : 1;
+    const int tx = (rows + nx - 1) / nx, ty = (JP->Y + ny - 1) / ny;
+    const long long capb = (long long)(tx + 2 * (k + 1)) * (ty + 2 * (k + 1));
+    if (tx >= 32 && ty >= 32 && tx <= 256 && ty <= 256 && capb <= 12LL * 1024 && capb < (1 << 16)) {
+      JP->TBX = tx;
+      JP->TBY = ty;
+      L->threads = 1024;
+      placed = true;
+    }
+  }
+  if (!placed) {
+    pick_tile_2d(JP->X, JP->Y, &JP->TBX, &JP->TBY);
+    L->threads = g_threads2d > 0 ? g_threads2d : 256;
+  }
   JP->tiles_y = (JP->Y + JP->TBY - 1) / JP->TBY;
   JP->RXM = JP->TBX + 2 * (k + 1);
   JP->RYM = JP->TBY + 2 * (k + 1);
   JP->h2 = h2;
-  *tiles = ((own_hi - own_lo + JP->TBX - 1) / JP->TBX) * JP->tiles_y;
-  *smem = (size_t)3 * JP->RXM * JP->RYM * sizeof(float);
-  if (*smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
-  if (cudaFuncSetAttribute(jacobi2d_tb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) != cudaSuccess)
+  L->tiles = ((own_hi - own_lo + JP->TBX - 1) / JP->TBX) * JP->tiles_y;
+  // the register cell lists cover every block's stencil rows x RY <= RXM x RYM
+  const long long cap = (long long)JP->RXM * JP->RYM;
+  L->cpt = cap <= 4LL * L->threads ? 4 : cap <= 6LL * L->threads ? 6 : cap <= 8LL * L->threads ? 8
+         : cap <= 12LL * L->threads ? 12 : 0;
+  L->smem = (size_t)3 * cap * sizeof(float);  // both kernels: two levels and the rhs per cell
+  if (L->smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
+  if (cap >= (1 << 16)) L->cpt = 0;  // the cell lists pack region indices in 16 bits
+  const void* kern = L->cpt == 4 ? (const void*)jacobi2d_cells_kernel<4>
+                   : L->cpt == 6 ? (const void*)jacobi2d_cells_kernel<6>
+                   : L->cpt == 8 ? (const void*)jacobi2d_cells_kernel<8>
+                   : L->cpt == 12 ? (const void*)jacobi2d_cells_kernel<12>
+                                  : (const void*)jacobi2d_tb_kernel;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L->smem) != cudaSuccess)
     return PDE_ERR_CUDA;
   return PDE_OK;
+}
+
+void launch_jacobi(const JacobiLaunch& L, cudaStream_t st, const float* pin, float* pout, const float* rhs,
+                   float* resid, const J2Params& JP, const PdeBCRules& R) {
+  switch (L.cpt) {
+    case 4: jacobi2d_cells_kernel<4><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
+    case 6: jacobi2d_cells_kernel<6><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
+    case 8: jacobi2d_cells_kernel<8><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
+    case 12: jacobi2d_cells_kernel<12><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
+    default: jacobi2d_tb_kernel<<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
+  }
 }
 
 }  // namespace
@@ -1078,9 +1124,8 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
   int k = prm->jacobi_per_pass > 0 ? prm->jacobi_per_pass : 10;
   if (k > iters && iters > 0) k = iters;
   J2Params JP;
-  int jtiles;
-  size_t jsmem;
-  rc = jacobi_setup(G, K.h2, k, 0, X, 0, X, &JP, &jtiles, &jsmem);
+  JacobiLaunch JL;
+  rc = jacobi_setup(G, K.h2, k, 0, X, 0, X, &JP, &JL);
   if (rc) return rc;
   for (int step = 0; step < nsteps; ++step) {
     ldc_predictor_kernel<<<grid2, 256, 0, st>>>(u, u_star, G, *u_rules, K, 0);
@@ -1091,8 +1136,7 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
       JP.k = (iters - done < k) ? (iters - done) : k;
       done += JP.k;
       JP.last = (done == iters);
-      jacobi2d_tb_kernel<<<jtiles, g_threads2d > 0 ? g_threads2d : 256, jsmem, st>>>(
-          src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
+      launch_jacobi(JL, st, src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
       float* t = src;
       src = dst;
       dst = t;
@@ -1230,14 +1274,12 @@ int pde_ldc_slab_step(int32_t phase, float* u, float* u_star, const float* p_in,
       // k sweeps invalidate k + 1 rows inward from a cut side of the held rows
       if ((cut_lo && lo - (nsweeps + 1) < off) || (cut_hi && hi + nsweeps + 1 > off + nloc)) return PDE_ERR_SHAPE;
       J2Params JP;
-      int jtiles;
-      size_t jsmem;
-      rc = jacobi_setup(G, K.h2, nsweeps, (int)lo, (int)hi, (int)off, (int)(off + nloc), &JP, &jtiles, &jsmem);
+      JacobiLaunch JL;
+      rc = jacobi_setup(G, K.h2, nsweeps, (int)lo, (int)hi, (int)off, (int)(off + nloc), &JP, &JL);
       if (rc) return rc;
       JP.k = nsweeps;
       JP.last = last ? 1 : 0;
-      jacobi2d_tb_kernel<<<jtiles, g_threads2d > 0 ? g_threads2d : 256, jsmem, st>>>(gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1),
-                                                     resid, JP, *p_rules);
+      launch_jacobi(JL, st, gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1), resid, JP, *p_rules);
       break;
     }
     default:

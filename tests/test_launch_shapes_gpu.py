@@ -118,7 +118,9 @@ def test_wave_balanced_tiles_at_514():
     _wave_check(514, 514, 20, 6, 7)
 
 
-@pytest.mark.parametrize("tile", ODD)
+# (64, 64, 256): more than 12 region cells per thread, the flat-walk Jacobi kernel;
+# the other shapes run the register cell-list kernel
+@pytest.mark.parametrize("tile", ODD + [(64, 64, 256)])
 def test_cavity_odd_tiles(tile, launch):
     n, steps, iters, k = 70, 3, 12, 4
     launch(*tile)
