@@ -375,7 +375,12 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
  * about one per SM, sides 16..64) and threads per block (256, 512, 1024;
  * 0 = automatic: for the wave and differentiable-heat kernels 1024 with up to one
  * tile per SM, 512 up to two, else 256; 512 for the fused heat rollout and the
- * weakly compressible step (which takes 256 or 512); 256 for the Jacobi sweeps). */
+ * weakly compressible step (which takes 256 or 512); 256 for the Jacobi sweeps).
+ * The Jacobi sweeps with both left automatic take one near-square tile per SM
+ * and 1024 threads when those tiles have sides of at least 32 and their region
+ * holds at most 12 cells per thread.  Any shape whose region holds at most 12
+ * cells per thread runs the register cell-list Jacobi kernel, others the
+ * flat-walk kernel (same results). */
 int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads);
 
 /* ---- batched rollouts (new: the reference advances every grid with its own
