@@ -152,13 +152,20 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
       HP.X = X; HP.Y = Y; HP.g = g; HP.N = 1;
       const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
       const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
-      const int SW = max(sy1 - sy0, 1), SC = max(sx1 - sx0, 0) * max(sy1 - sy0, 0);
-      const int dq = nt / SW, dr = nt - dq * SW;
+      const int tlx0 = bx0 - rx0, tly0 = by0 - ry0;  // the tile in region coordinates
       for (int s = 0; s < ks; ++s) {
         bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, dx32);
+        // Step s only has to update the stencil cells within R (ks - 1 - s) + 1 of
+        // the tile (the boundary fills read inward): the stencil rectangle cut to
+        // that box; the cells outside it keep stale values nobody reads.
+        const int reach = R * (ks - 1 - s) + 1;
+        const int qx0 = max(sx0, tlx0 - reach), qx1 = min(sx1, tlx0 + OX + reach);
+        const int qy0 = max(sy0, tly0 - reach), qy1 = min(sy1, tly0 + OY + reach);
+        const int SW = max(qy1 - qy0, 1), SC = max(qx1 - qx0, 0) * max(qy1 - qy0, 0);
+        const int dq = nt / SW, dr = nt - dq * SW;
         int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
         for (int c = threadIdx.x; c < SC; c += nt) {
-          const int i = (sx0 + lx) * RY + sy0 + ly;
+          const int i = (qx0 + lx) * RY + qy0 + ly;
           const float u2 = A[i];
           float acc = 0.0f;
 #pragma unroll
@@ -204,12 +211,17 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
       // computed rectangle: inside the ring, one cell away from the region's edges
       const int cx0 = max(g + 1, rx0 + 1) - rx0, cx1 = min(X - 1 - g, rx0 + RX - 1) - rx0;
       const int cy0 = max(g + 1, ry0 + 1) - ry0, cy1 = min(Y - 1 - g, ry0 + RY - 1) - ry0;
-      const int CW = max(cy1 - cy0, 1), CC = max(cx1 - cx0, 0) * max(cy1 - cy0, 0);
-      const int dq = nt / CW, dr = nt - dq * CW;
+      const int tlx0 = bx0 - rx0, tly0 = by0 - ry0;  // the tile in region coordinates
       for (int s = 0; s < ks; ++s) {
+        // step s only has to update the cells within ks - 1 - s of the tile
+        const int reach = ks - 1 - s;
+        const int qx0 = max(cx0, tlx0 - reach), qx1 = min(cx1, tlx0 + OX + reach);
+        const int qy0 = max(cy0, tly0 - reach), qy1 = min(cy1, tly0 + OY + reach);
+        const int CW = max(qy1 - qy0, 1), CC = max(qx1 - qx0, 0) * max(qy1 - qy0, 0);
+        const int dq = nt / CW, dr = nt - dq * CW;
         int lx = (int)threadIdx.x / CW, ly = (int)threadIdx.x - lx * CW;
         for (int c = threadIdx.x; c < CC; c += nt) {
-          const int i = (cx0 + lx) * RY + cy0 + ly;
+          const int i = (qx0 + lx) * RY + qy0 + ly;
           float acc = 0.0f;  // Laplacian, alpha 1 (FDM/kernel/laplacian.py:40-46 order)
           acc = add(acc, mul(w[0], B0[i - RY]));
           acc = add(acc, mul(w[1], B0[i]));
