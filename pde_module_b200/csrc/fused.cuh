@@ -9,6 +9,8 @@
 // component, evaluated on the pre-boundary field at the interior neighbour
 // (adj = node + inc).  All other cells keep the input value.
 #pragma once
+#include <type_traits>
+
 #include "common.cuh"
 #include "generic.cuh"
 
@@ -312,6 +314,109 @@ __global__ void __launch_bounds__(1024) heat2d_tb_kernel(const float* __restrict
   RectWalk wo(onrow, nt);
   for (int i = threadIdx.x; i < (ox1 - bx0) * onrow; i += nt, wo.next())
     out[((size_t)(bx0 + wo.row) * P.Y + by0) * N + wo.col] = A[(bx0 + wo.row - rx0) * nrow + (by0 - ry0) * N + wo.col];
+}
+
+// The same passes for a one-component field with register cell lists (as the
+// wave and Jacobi kernels): the region interleaves the two levels (3 floats per
+// cell, an odd stride: no bank conflicts), each thread's region cells are fixed
+// for the pass (slots q = threadIdx.x + c * blockDim.x over the region's rows),
+// each with one packed word (region index in the low 16 bits, distance from the
+// tile above) and a bit for "stencil cell".  Step s reads level s & 1, writes the
+// other, and updates the cells within R (k - 1 - s) + 1 of the tile: stencil
+// cells by the reference's sum, the others (ghosts, cut edges) copied through.
+// Same arithmetic and order per cell as heat2d_tb_kernel<R, 1, RAMP>; needs
+// RXM x RYM <= MAXC * blockDim.x and < 2^16.
+template <int R, int MAXC, bool RAMP>
+__global__ void __launch_bounds__(1024) heat2d_cells_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                            const H2Params P, const PdeBCRules Rl) {
+  extern __shared__ __align__(16) float sm[];
+  __shared__ PdeBCRules SR;  // RAMP only: the rules with the current step's group values
+  if (RAMP && threadIdx.x == 0) SR = Rl;
+  constexpr int NB = 3;  // per region cell: level 0, level 1, (unused)
+  const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
+  const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
+  const int H = P.k * R + 1;
+  const int rx0 = max(bx0 - H, 0), rx1 = min(bx0 + P.TBX + H, P.X);
+  const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
+  const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
+  const int nt = (int)blockDim.x;
+  {
+    RectWalk wk(RY, nt);
+    for (int i = threadIdx.x; i < RC; i += nt, wk.next())
+      cp_async4(sm + NB * i, in + (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col, true);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int g = P.g;
+  // stencil cells whose R neighbours along both axes are inside the region
+  const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(P.X - g, rx0 + RX - R) - rx0;
+  const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(P.Y - g, ry0 + RY - R) - ry0;
+  const int ox1 = min(bx0 + P.TBX, P.X), oy1 = min(by0 + P.TBY, P.Y);
+  // the tile in region coordinates (inclusive bounds)
+  const int tlx0 = bx0 - rx0, tlx1 = ox1 - 1 - rx0, tly0 = by0 - ry0, tly1 = oy1 - 1 - ry0;
+  int key[MAXC];      // region index | distance from the tile << 16; idle slots: INT_MAX
+  unsigned sten = 0;  // bit c: slot c is a stencil cell
+  {
+    RectWalk wk(RY, nt);
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      key[c] = 0x7fffffff;
+      if ((int)threadIdx.x + c * nt < RC) {
+        const int lx = wk.row, ly = wk.col;
+        const int d = max(max(max(tlx0 - lx, lx - tlx1), max(tly0 - ly, ly - tly1)), 0);
+        key[c] = (lx * RY + ly) | (d << 16);
+        if (lx >= sx0 && lx < sx1 && ly >= sy0 && ly < sy1) sten |= 1u << c;
+      }
+      wk.next();
+    }
+  }
+  const int rs = NB * RY;
+  auto step = [&](auto PAR, int s) {
+    constexpr int p = decltype(PAR)::value;  // reads level p, writes level 1 - p
+    if constexpr (RAMP) {
+      // every read of SR's values in the previous step came before its last barrier
+      const int gi = (int)threadIdx.x;
+      if (gi < Rl.ngroups && Rl.group[gi].func == PDE_BC_FUNC_RAMP) {
+        const float t = step_time(P.t0, P.tstep, P.n0 + s);
+        SR.group[gi].value = bc_value(PDE_BC_FUNC_RAMP, Rl.group[gi].value, Rl.group[gi].t_max, &t);
+      }
+      __syncthreads();
+      bc_fill_region<1, NB>(sm + p, P, SR, rx0, RX, ry0, RY, Rl.dx32);
+    } else {
+      bc_fill_region<1, NB>(sm + p, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    }
+    // Only the cells within R (k - 1 - s) + 1 of the tile can reach the tile's
+    // result (the boundary fills read inward, never farther out).
+    const int lim = (R * (P.k - 1 - s) + 2) << 16;  // dist <= reach  <=>  key < lim
+#pragma unroll
+    for (int c = 0; c < MAXC; ++c) {
+      if (key[c] >= lim) continue;
+      float* pc = sm + NB * (key[c] & 0xffff) + p;
+      const float u2 = pc[0];
+      float res = u2;
+      if ((sten >> c) & 1u) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], pc[(t - R) * rs]));
+#pragma unroll
+        for (int t = 0; t < 2 * R + 1; ++t) acc = add(acc, mul(P.w[t], pc[(t - R) * NB]));
+        res = add(u2, mul(P.dt, mul(P.alpha, acc)));
+      }
+      pc[1 - 2 * p] = res;  // the other level of the same cell
+    }
+    __syncthreads();
+  };
+  for (int s = 0; s < P.k; s += 2) {
+    step(std::integral_constant<int, 0>{}, s);
+    if (s + 1 < P.k) step(std::integral_constant<int, 1>{}, s + 1);
+  }
+  // The ghost cells of the result hold the last step's boundary-filled values
+  // (non-stencil cells copy their filled value through).
+  const int nw = P.k & 1;  // the level the last step wrote
+  const int OX = ox1 - bx0, OY = oy1 - by0;
+  RectWalk wo(OY, nt);
+  for (int i = threadIdx.x; i < OX * OY; i += nt, wo.next())
+    out[(size_t)(bx0 + wo.row) * P.Y + by0 + wo.col] = sm[NB * ((tlx0 + wo.row) * RY + tly0 + wo.col) + nw];
 }
 
 }  // namespace pde

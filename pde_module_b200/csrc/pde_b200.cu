@@ -563,6 +563,24 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
       P.t0 = t0; P.tstep = tstep; P.n0 = done;
       const size_t smem = (size_t)2 * P.RXM * P.RYM * ncomp * sizeof(float);
       if (smem > 227 * 1024 - sizeof(PdeBCRules)) return PDE_ERR_TOO_LARGE;
+      // one component and at most 8 region cells per thread: the register cell-list kernel
+      const long long cap = (long long)P.RXM * P.RYM;
+      const int cpt = (ncomp == 1 && cap < (1 << 16)) ? (cap <= 4LL * threads ? 4 : cap <= 8LL * threads ? 8 : 0) : 0;
+      const size_t smem_c = (size_t)3 * cap * sizeof(float);
+      if (cpt > 0 && smem_c <= 227 * 1024 - sizeof(PdeBCRules)) {
+#define PDE_H2C(RR, CC)                                                                                    \
+  do {                                                                                                     \
+    auto kern = rules->has_ramp ? heat2d_cells_kernel<RR, CC, true> : heat2d_cells_kernel<RR, CC, false>;  \
+    PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c)); \
+    kern<<<tiles, threads, smem_c, st>>>(src, dst, P, *rules);                                             \
+  } while (0)
+        if (R == 1) {
+          if (cpt == 4) PDE_H2C(1, 4); else PDE_H2C(1, 8);
+        } else {
+          if (cpt == 4) PDE_H2C(2, 4); else PDE_H2C(2, 8);
+        }
+#undef PDE_H2C
+      } else {
 #define PDE_H2(RR, NN)                                                                                  \
   do {                                                                                                  \
     auto kern = rules->has_ramp ? heat2d_tb_kernel<RR, NN, true> : heat2d_tb_kernel<RR, NN, false>;      \
@@ -585,6 +603,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
         }
       }
 #undef PDE_H2
+      }
     } else {
       const int64_t total = G.n[0] * G.n[1] * G.n[2] * ncomp;
       // one step per launch: time-dependent group values are set in a copy of the rules
