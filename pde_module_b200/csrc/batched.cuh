@@ -153,8 +153,10 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
       const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(X - g, rx0 + RX - R) - rx0;
       const int sy0 = max(g, ry0 + R) - ry0, sy1 = min(Y - g, ry0 + RY - R) - ry0;
       const int tlx0 = bx0 - rx0, tly0 = by0 - ry0;  // the tile in region coordinates
+      BcPlan<2> bp;
+      bc_plan(bp, HP, rx0, RX, ry0, RY);
       for (int s = 0; s < ks; ++s) {
-        bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, dx32);
+        bc_fill_planned<1, 1>(A, bp, HP, Rl, rx0, RX, ry0, RY, dx32);
         // Step s only has to update the stencil cells within R (ks - 1 - s) + 1 of
         // the tile (the boundary fills read inward): the stencil rectangle cut to
         // that box; the cells outside it keep stale values nobody reads.

@@ -227,6 +227,118 @@ __device__ __forceinline__ void bc_fill_region(float* A, const H2Params& P, cons
   __syncthreads();
 }
 
+// The boundary-fill work of one thread for a region fixed over many fills (a
+// launch, or a batched item): up to E ghost cells (region index, the partner two
+// cells inward, boundary class, axis, side) and up to E node cells (region index,
+// class), found once with the enumeration of bc_fill_region, so a fill needs no
+// index arithmetic.  Region indices are packed in 16 bits; regions of 2^16 cells
+// or more, or with more strip cells than E per thread, use bc_fill_region.
+template <int E>
+struct BcPlan {
+  unsigned gh[E];  // ghost | partner << 16; ~0u: none
+  int gm[E];       // class K | axis << 5 | (side low ? 1 : 0) << 6
+  unsigned nd[E];  // node | K << 16; ~0u: none
+  int mode;        // 0: nothing to fill, 1: planned, 2: bc_fill_region (block-uniform)
+};
+
+template <int E>
+__device__ __forceinline__ void bc_plan(BcPlan<E>& pl, const H2Params& P, int rx0, int RX, int ry0, int RY) {
+  const int g = P.g, X = P.X, Y = P.Y;
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    pl.gh[i] = ~0u;
+    pl.gm[i] = 0;
+    pl.nd[i] = ~0u;
+  }
+  pl.mode = 0;
+  if (rx0 > g && rx0 + RX < X - g && ry0 > g && ry0 + RY < Y - g) return;
+  const int nthr = blockDim.x, tid = threadIdx.x;
+  const int ylo = max(g, ry0), yhi = min(Y - g, ry0 + RY);
+  const int xlo = max(g, rx0), xhi = min(X - g, rx0 + RX);
+  const int ny = max(0, yhi - ylo), nx = max(0, xhi - xlo);
+  const int total = 2 * ny + 2 * nx;
+  if (total > E * nthr || RX * RY >= (1 << 16) - 1) {
+    pl.mode = 2;
+    return;
+  }
+  pl.mode = 1;
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int e = tid + i * nthr;
+    if (e >= total) continue;
+    int gx, gy, ax, inc, x, y;  // ghost (gx, gy) and node (x, y) of strip element e
+    if (e < 2 * ny) {
+      const int side = e / ny;
+      gy = ylo + (e - side * ny);
+      gx = side == 0 ? g - 1 : X - g;
+      inc = side == 0 ? 1 : -1;
+      ax = 0;
+      y = gy;
+      x = side == 0 ? g : X - g - 1;
+    } else {
+      const int e2 = e - 2 * ny;
+      const int side = e2 / nx;
+      gx = xlo + (e2 - side * nx);
+      gy = side == 0 ? g - 1 : Y - g;
+      inc = side == 0 ? 1 : -1;
+      ax = 1;
+      x = gx;
+      y = side == 0 ? g : Y - g - 1;
+    }
+    const int px = gx + (ax == 0 ? inc : 0), py = gy + (ax == 1 ? inc : 0);
+    const int qx = px + (ax == 0 ? inc : 0), qy = py + (ax == 1 ? inc : 0);
+    if (!(gx < rx0 || gx >= rx0 + RX || gy < ry0 || gy >= ry0 + RY) &&
+        !(qx < rx0 || qx >= rx0 + RX || qy < ry0 || qy >= ry0 + RY)) {
+      const int K = node_class_axis(px, X, g, true) * 9 + node_class_axis(py, Y, g, true) * 3 + 1;
+      pl.gh[i] = (unsigned)((gx - rx0) * RY + (gy - ry0)) | ((unsigned)((qx - rx0) * RY + (qy - ry0)) << 16);
+      pl.gm[i] = K | (ax << 5) | ((inc > 0 ? 1 : 0) << 6);
+    }
+    if (!(x < rx0 || x >= rx0 + RX || y < ry0 || y >= ry0 + RY)) {
+      const int K = node_class_axis(x, X, g, true) * 9 + node_class_axis(y, Y, g, true) * 3 + 1;
+      pl.nd[i] = (unsigned)((x - rx0) * RY + (y - ry0)) | ((unsigned)K << 16);
+    }
+  }
+}
+
+// bc_fill_region by a plan: the same cells, values and order (ghosts, barrier,
+// nodes, barrier).
+template <int N, int S, int E>
+__device__ __forceinline__ void bc_fill_planned(float* A, const BcPlan<E>& pl, const H2Params& P,
+                                                const PdeBCRules& Rl, int rx0, int RX, int ry0, int RY, float dx32) {
+  if (pl.mode == 0) return;
+  if (pl.mode == 2) {
+    bc_fill_region<N, S>(A, P, Rl, rx0, RX, ry0, RY, dx32);
+    return;
+  }
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    if (pl.gh[i] == ~0u) continue;
+    const int dst = (int)(pl.gh[i] & 0xffffu), src = (int)(pl.gh[i] >> 16);
+    const int K = pl.gm[i] & 31, ax = (pl.gm[i] >> 5) & 1, inc = ((pl.gm[i] >> 6) & 1) ? 1 : -1;
+#pragma unroll
+    for (int v = 0; v < N; ++v) {
+      const int gi = Rl.ghost_group[K][ax][v];
+      if (gi < 0) continue;
+      const float a = A[src * S + v];
+      A[dst * S + v] = ghost_value(Rl, gi, inc, a, dx32);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    if (pl.nd[i] == ~0u) continue;
+    const int dst = (int)(pl.nd[i] & 0xffffu), K = (int)(pl.nd[i] >> 16);
+    const int gi = Rl.node_group[K];
+    if (gi < 0) continue;
+    const uint32_t m = Rl.group[gi].comp_mask;
+    const float val = Rl.group[gi].value;
+#pragma unroll
+    for (int v = 0; v < N; ++v)
+      if ((m >> v) & 1u) A[dst * S + v] = val;
+  }
+  __syncthreads();
+}
+
 // k fused steps on a 2D grid (X, Y, 1, N) per pass.  Tiles cover the whole
 // array (ghosts included); the smem region is the tile grown by H = k*R + 1
 // cells on each side (clipped to the array).  Values invalidated by the
@@ -371,6 +483,8 @@ __global__ void __launch_bounds__(1024) heat2d_cells_kernel(const float* __restr
     }
   }
   const int rs = NB * RY;
+  BcPlan<1> bp;
+  bc_plan(bp, P, rx0, RX, ry0, RY);
   auto step = [&](auto PAR, int s) {
     constexpr int p = decltype(PAR)::value;  // reads level p, writes level 1 - p
     if constexpr (RAMP) {
@@ -381,9 +495,9 @@ __global__ void __launch_bounds__(1024) heat2d_cells_kernel(const float* __restr
         SR.group[gi].value = bc_value(PDE_BC_FUNC_RAMP, Rl.group[gi].value, Rl.group[gi].t_max, &t);
       }
       __syncthreads();
-      bc_fill_region<1, NB>(sm + p, P, SR, rx0, RX, ry0, RY, Rl.dx32);
+      bc_fill_planned<1, NB>(sm + p, bp, P, SR, rx0, RX, ry0, RY, Rl.dx32);
     } else {
-      bc_fill_region<1, NB>(sm + p, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
+      bc_fill_planned<1, NB>(sm + p, bp, P, Rl, rx0, RX, ry0, RY, Rl.dx32);
     }
     // Only the cells within R (k - 1 - s) + 1 of the tile can reach the tile's
     // result (the boundary fills read inward, never farther out).

@@ -343,11 +343,13 @@ __global__ void __launch_bounds__(1024) jacobi2d_cells_kernel(const float* __res
   }
   const int rs = NB * RY;
   float sq = 0.0f;
+  BcPlan<1> bp;
+  bc_plan(bp, HP, rx0, RX, ry0, RY);
   // Sweep s only has to update the stencil cells within (k - 1 - s) + 1 of the
   // tile (the boundary fills read inward): those with dist <= k - s.
   auto sweep = [&](auto PAR, int s) {
     constexpr int p = decltype(PAR)::value;  // reads level p, writes level 1 - p
-    bc_fill_region<1, NB>(sm + p, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);
+    bc_fill_planned<1, NB>(sm + p, bp, HP, Rp, rx0, RX, ry0, RY, Rp.dx32);
     const bool acc_res = P.last && s == P.k - 1;
     const int lim = (P.k - s + 1) << 16;  // dist <= k - s  <=>  key < lim
 #pragma unroll

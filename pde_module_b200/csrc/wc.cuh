@@ -63,6 +63,8 @@ __global__ void __launch_bounds__(512) wc_rk2_kernel(const float* __restrict__ m
   hp.X = X;
   hp.Y = Y;
   hp.g = g;
+  BcPlan<2> bp;               // one region for both fields and all four fills
+  bc_plan(bp, hp, rx0, RX, ry0, RY);
   wc_region(RC, RY, [&](int i, int lx, int ly) {
     const size_t c = (size_t)(rx0 + lx) * Y + ry0 + ly;
     cp_async4(M0 + 2 * i, m_in + 2 * c, true);
@@ -87,8 +89,8 @@ __global__ void __launch_bounds__(512) wc_rk2_kernel(const float* __restrict__ m
       U[2 * i + 1] = __fdiv_rn(M[2 * i + 1], Rh[i]);
     });
     __syncthreads();
-    bc_fill_region<2>(U, hp, Ru, rx0, RX, ry0, RY, Ru.dx32);
-    bc_fill_region<1>(Rh, hp, Rr, rx0, RX, ry0, RY, Rr.dx32);
+    bc_fill_planned<2, 2>(U, bp, hp, Ru, rx0, RX, ry0, RY, Ru.dx32);
+    bc_fill_planned<1, 1>(Rh, bp, hp, Rr, rx0, RX, ry0, RY, Rr.dx32);
     __syncthreads();
     wc_region(RC, RY, [&](int i, int, int) {
       M[2 * i] = mul(Rh[i], U[2 * i]);
