@@ -64,8 +64,10 @@ __device__ __forceinline__ float* heat_field_steps(const HAParams& P, const PdeB
   const int nt = (int)blockDim.x;
   const int dq = nt / SW, dr = nt - dq * SW;
   const int tx0 = bx0 - rx0 - sx0, ty0 = by0 - ry0 - sy0;  // the tile in rectangle coordinates
+  BcPlan<2> bp;  // the region is the same for every step of the pass
+  bc_plan(bp, HP, rx0, RX, ry0, RY);
   for (int s = 0; s < P.k; ++s) {
-    bc_fill_region<1>(A, HP, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    bc_fill_planned<1, 1>(A, bp, HP, Rl, rx0, RX, ry0, RY, Rl.dx32);
     float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
     int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
     for (int c = threadIdx.x; c < SC; c += nt) {
@@ -155,13 +157,31 @@ __device__ __forceinline__ bool bc_overwritten(const PdeBCRules& Rl, int x, int 
   return false;
 }
 
-// mu of the ghost across node (px, py) on `axis`, folded into v with its sign.
-__device__ __forceinline__ float bt_ghost(const PdeBCRules& Rl, float v, float mG, int px, int py, int axis, int X,
-                                          int Y, int g) {
+// How the mu of the ghost across node (px, py) on `axis` folds into its partner:
+// 0 not at all (no ghost group), 1 subtracted (Dirichlet), 2 added.
+__device__ __forceinline__ int bt_code(const PdeBCRules& Rl, int px, int py, int axis, int X, int Y, int g) {
   const int K = node_class_axis(px, X, g, true) * 9 + node_class_axis(py, Y, g, true) * 3 + 1;
   const int gi = Rl.ghost_group[K][axis][0];
-  if (gi < 0) return v;
-  return Rl.group[gi].type == PDE_BC_DIRICHLET ? sub(v, mG) : add(v, mG);
+  if (gi < 0) return 0;
+  return Rl.group[gi].type == PDE_BC_DIRICHLET ? 1 : 2;
+}
+
+__device__ __forceinline__ float bt_fold(float v, float mG, int code) {
+  return code == 1 ? sub(v, mG) : add(v, mG);
+}
+
+// The boundary role of region cell (x, y), fixed for a launch: bit 0 overwritten
+// by the fill (bc_overwritten), bits 1-2 / 3-4 / 5-6 / 7-8 the fold codes of the
+// x-low, x-high, y-low and y-high ghost whose partner it is, bit 9 stencil cell.
+__device__ __forceinline__ int bt_flags(const PdeBCRules& Rl, int x, int y, int X, int Y, int g) {
+  int f = bc_overwritten(Rl, x, y, X, Y, g) ? 1 : 0;
+  const bool yin = y >= g && y < Y - g, xin = x >= g && x < X - g;
+  if (yin && x == g + 1) f |= bt_code(Rl, g, y, 0, X, Y, g) << 1;
+  if (yin && x == X - g - 2) f |= bt_code(Rl, X - g - 1, y, 0, X, Y, g) << 3;
+  if (xin && y == g + 1) f |= bt_code(Rl, x, g, 1, X, Y, g) << 5;
+  if (xin && y == Y - g - 2) f |= bt_code(Rl, x, Y - g - 1, 1, X, Y, g) << 7;
+  if (heat_stencil_cell(x, y, X, Y, g)) f |= 1 << 9;
+  return f;
 }
 
 template <int R>
@@ -190,6 +210,8 @@ __global__ void __launch_bounds__(1024) heat2d_adj_kernel(const float* __restric
   // S^n of the tile for the current and the next step (two slots): the next
   // step's values are copied in (cp.async) while the current step computes
   float* GL = GA + P.TBX * P.TBY;
+  // bt_flags of the region's cells (regions that touch the boundary)
+  int* FL = reinterpret_cast<int*>(GL + 2 * P.TBX * P.TBY);
   const int OT = OX * OY;
   auto fetch_S = [&](int s, int slot) {
     const float* Sn = P.lsts + (size_t)(P.ntop - s) * P.cells;
@@ -263,6 +285,12 @@ __global__ void __launch_bounds__(1024) heat2d_adj_kernel(const float* __restric
     Zc = Zn;
     Zn = t;
   }
+  if (!interior) {
+    RectWalk wk(RY, (int)blockDim.x);
+    for (int i = threadIdx.x; i < RC; i += blockDim.x, wk.next())
+      FL[i] = bt_flags(Rl, rx0 + wk.row, ry0 + wk.col, X, Y, g);
+    __syncthreads();
+  }
   for (int s = 0; s < P.k && !interior; ++s) {
     if (s + 1 < P.k) fetch_S(s + 1, (s + 1) & 1);  // its slot was last read in step s-1
     const float* Sg = GL + (s & 1) * OT;
@@ -285,7 +313,7 @@ __global__ void __launch_bounds__(1024) heat2d_adj_kernel(const float* __restric
       const float l = Lm[i];
       M[i] = add(l, acc);
       const int x = rx0 + lx, y = ry0 + ly;
-      if (x >= bx0 && x < ox1 && y >= by0 && y < oy1 && heat_stencil_cell(x, y, X, Y, g)) {
+      if (x >= bx0 && x < ox1 && y >= by0 && y < oy1 && ((FL[i] >> 9) & 1)) {
         const int gi = (x - bx0) * OY + (y - by0);
         GA[gi] = add(GA[gi], mul(l, mul(dt, Sg[gi])));
       }
@@ -295,22 +323,16 @@ __global__ void __launch_bounds__(1024) heat2d_adj_kernel(const float* __restric
     }
     __syncthreads();
     // lam = B^T(mu); z for the next step
-    lx = lxs;
-    ly = lys;
     for (int i = threadIdx.x; i < RC; i += blockDim.x) {
-      const int x = rx0 + lx, y = ry0 + ly;
-      float v = bc_overwritten(Rl, x, y, X, Y, g) ? 0.0f : M[i];
-      const bool yin = y >= g && y < Y - g, xin = x >= g && x < X - g;
+      const int f = FL[i];
+      float v = (f & 1) ? 0.0f : M[i];
       // the ghost of each pair lies in the region whenever its partner does (edge snapping)
-      if (yin && x == g + 1) v = bt_ghost(Rl, v, M[i - 2 * RY], g, y, 0, X, Y, g);
-      if (yin && x == X - g - 2) v = bt_ghost(Rl, v, M[i + 2 * RY], X - g - 1, y, 0, X, Y, g);
-      if (xin && y == g + 1) v = bt_ghost(Rl, v, M[i - 2], x, g, 1, X, Y, g);
-      if (xin && y == Y - g - 2) v = bt_ghost(Rl, v, M[i + 2], x, Y - g - 1, 1, X, Y, g);
+      if (f & (3 << 1)) v = bt_fold(v, M[i - 2 * RY], (f >> 1) & 3);
+      if (f & (3 << 3)) v = bt_fold(v, M[i + 2 * RY], (f >> 3) & 3);
+      if (f & (3 << 5)) v = bt_fold(v, M[i - 2], (f >> 5) & 3);
+      if (f & (3 << 7)) v = bt_fold(v, M[i + 2], (f >> 7) & 3);
       Lm[i] = v;
-      Z[i] = heat_stencil_cell(x, y, X, Y, g) ? mul(dt, mul(AL[i], v)) : 0.0f;
-      lx += dq;
-      ly += dr;
-      if (ly >= RY) { ly -= RY; ++lx; }
+      Z[i] = ((f >> 9) & 1) ? mul(dt, mul(AL[i], v)) : 0.0f;
     }
     cp_async_wait_all();  // this thread's copies of the next step's S; the barrier publishes them
     __syncthreads();

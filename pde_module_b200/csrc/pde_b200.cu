@@ -780,7 +780,8 @@ int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, co
   const int R = G.order / 2;
   const int H = k * R;
   P.RC = (P.TBX + 2 * H + 2 * (G.g + 2)) * (P.TBY + 2 * H + 2 * (G.g + 2));
-  const size_t smem = ((size_t)4 * P.RC + (size_t)3 * P.TBX * P.TBY) * sizeof(float);
+  // four region fields, the boundary flags of the region, the tile's gradient and two S planes
+  const size_t smem = ((size_t)5 * P.RC + (size_t)3 * P.TBX * P.TBY) * sizeof(float);
   if (smem > 227 * 1024) return PDE_ERR_TOO_LARGE;
   auto kern = R == 1 ? heat2d_adj_kernel<1> : heat2d_adj_kernel<2>;
   PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
