@@ -16,6 +16,15 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
 // Wait for this thread's cp.async copies (the block still needs a barrier before others read them).
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start while the previous kernel of its stream runs.
+// pdl_launch_dependents lets the next kernel be scheduled (it still waits);
+// pdl_wait blocks until the previous kernel has completed and its writes are
+// visible: every global access to data another launch reads or writes comes
+// after it.  Both are no-ops for kernels launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 // Walk of a row-major (rows x W) rectangle by a block: cell c = tid, tid + nt, ...
 // as (row, col), advanced without division.
 struct RectWalk {

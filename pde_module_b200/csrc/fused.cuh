@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(1024) heat2d_tb_kernel(const float* __restrict
 template <int R, int MAXC, bool RAMP>
 __global__ void __launch_bounds__(1024) heat2d_cells_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                             const H2Params P, const PdeBCRules Rl) {
+  pdl_launch_dependents();  // the next pass may be scheduled; it waits for this one
   extern __shared__ __align__(16) float sm[];
   __shared__ PdeBCRules SR;  // RAMP only: the rules with the current step's group values
   if (RAMP && threadIdx.x == 0) SR = Rl;
@@ -452,13 +453,6 @@ __global__ void __launch_bounds__(1024) heat2d_cells_kernel(const float* __restr
   const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
   const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
   const int nt = (int)blockDim.x;
-  {
-    RectWalk wk(RY, nt);
-    for (int i = threadIdx.x; i < RC; i += nt, wk.next())
-      cp_async4(sm + NB * i, in + (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col, true);
-  }
-  cp_async_wait_all();
-  __syncthreads();
   const int g = P.g;
   // stencil cells whose R neighbours along both axes are inside the region
   const int sx0 = max(g, rx0 + R) - rx0, sx1 = min(P.X - g, rx0 + RX - R) - rx0;
@@ -485,6 +479,14 @@ __global__ void __launch_bounds__(1024) heat2d_cells_kernel(const float* __restr
   const int rs = NB * RY;
   BcPlan<1> bp;
   bc_plan(bp, P, rx0, RX, ry0, RY);
+  pdl_wait();  // the previous pass's output (this pass's input) is complete
+  {
+    RectWalk wk(RY, nt);
+    for (int i = threadIdx.x; i < RC; i += nt, wk.next())
+      cp_async4(sm + NB * i, in + (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col, true);
+  }
+  cp_async_wait_all();
+  __syncthreads();
   auto step = [&](auto PAR, int s) {
     constexpr int p = decltype(PAR)::value;  // reads level p, writes level 1 - p
     if constexpr (RAMP) {

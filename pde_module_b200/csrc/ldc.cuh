@@ -291,6 +291,7 @@ __global__ void __launch_bounds__(1024) jacobi2d_cells_kernel(const float* __res
                                                               const float* __restrict__ rhs,
                                                               float* __restrict__ resid, const J2Params P,
                                                               const PdeBCRules Rp) {
+  pdl_launch_dependents();  // the next pass may be scheduled; it waits for this one
   extern __shared__ __align__(16) float sm[];
   constexpr int NB = 3;  // per region cell: level 0, level 1, rhs
   const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
@@ -300,17 +301,6 @@ __global__ void __launch_bounds__(1024) jacobi2d_cells_kernel(const float* __res
   const int ry0 = max(by0 - H, 0), ry1 = min(by0 + P.TBY + H, P.Y);
   const int RX = rx1 - rx0, RY = ry1 - ry0, RC = RX * RY;
   const int nt = (int)blockDim.x;
-  {
-    RectWalk wk(RY, nt);
-    for (int i = threadIdx.x; i < RC; i += nt, wk.next()) {
-      const size_t gi = (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col;
-      cp_async4(sm + NB * i, pin + gi, true);
-      cp_async4(sm + NB * i + 1, pin + gi, true);
-      cp_async4(sm + NB * i + 2, rhs + gi, true);
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
   H2Params HP;
   HP.X = P.X; HP.Y = P.Y; HP.g = P.g; HP.N = 1;
   const int g = P.g;
@@ -328,15 +318,12 @@ __global__ void __launch_bounds__(1024) jacobi2d_cells_kernel(const float* __res
 #pragma unroll
     for (int c = 0; c < MAXC; ++c) {
       key[c] = 0x7fffffff;
-      hr[c] = 0.0f;
       if ((int)threadIdx.x + c * nt < n && wk.col >= sy0 && wk.col < sy1) {
         const int lx = sx0 + wk.row, ly = wk.col;
-        const int r = lx * RY + ly;
         const int ox = lx - tlx, oy = ly - tly;
         const int d = max(max(max(-ox, ox - (tw - 1)), max(-oy, oy - (th - 1))), 0);
-        key[c] = r | (d << 16);
+        key[c] = (lx * RY + ly) | (d << 16);
         if (ox >= 0 && ox < tw && oy >= 0 && oy < th) tile |= 1u << c;
-        hr[c] = mul(P.h2, sm[NB * r + 2]);
       }
       wk.next();
     }
@@ -345,6 +332,21 @@ __global__ void __launch_bounds__(1024) jacobi2d_cells_kernel(const float* __res
   float sq = 0.0f;
   BcPlan<1> bp;
   bc_plan(bp, HP, rx0, RX, ry0, RY);
+  pdl_wait();  // the previous pass's pressure (this pass's input) is complete
+  {
+    RectWalk wk(RY, nt);
+    for (int i = threadIdx.x; i < RC; i += nt, wk.next()) {
+      const size_t gi = (size_t)(rx0 + wk.row) * P.Y + ry0 + wk.col;
+      cp_async4(sm + NB * i, pin + gi, true);
+      cp_async4(sm + NB * i + 1, pin + gi, true);
+      cp_async4(sm + NB * i + 2, rhs + gi, true);
+    }
+  }
+  cp_async_wait_all();
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < MAXC; ++c)  // h^2 rhs of the thread's cells (the same product every sweep)
+    hr[c] = key[c] != 0x7fffffff ? mul(P.h2, sm[NB * (key[c] & 0xffff) + 2]) : 0.0f;
   // Sweep s only has to update the stencil cells within (k - 1 - s) + 1 of the
   // tile (the boundary fills read inward): those with dist <= k - s.
   auto sweep = [&](auto PAR, int s) {

@@ -42,6 +42,24 @@ int g_threads2d = 0;
 // A 2D tile count just above m x SMs (m = 1, 2) leaves a short tail wave in which
 // a few SMs run a second tile while the rest wait: enlarge the tiles slightly
 // (at most two fewer tiles per axis, sides up to 256) so the count drops to m x SMs.
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while the previous kernel of the stream runs; it calls pdl_wait before any
+// global access to data another launch reads or writes.
+template <typename... KArgs, typename... Args>
+int launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...) == cudaSuccess ? PDE_OK : PDE_ERR_CUDA;
+}
+
 void balance_tiles(int X, int Y, int* tbx, int* tby) {
   const long long sms = sm_count();
   const long long nx = (X + *tbx - 1) / *tbx, ny = (Y + *tby - 1) / *tby;
@@ -572,7 +590,8 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
   do {                                                                                                     \
     auto kern = rules->has_ramp ? heat2d_cells_kernel<RR, CC, true> : heat2d_cells_kernel<RR, CC, false>;  \
     PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c)); \
-    kern<<<tiles, threads, smem_c, st>>>(src, dst, P, *rules);                                             \
+    const int lrc = launch_pdl(kern, tiles, threads, smem_c, st, src, dst, P, *rules);                     \
+    if (lrc) return lrc;                                                                                   \
   } while (0)
         if (R == 1) {
           if (cpt == 4) PDE_H2C(1, 4); else PDE_H2C(1, 8);
@@ -1112,14 +1131,17 @@ int jacobi_setup(const Geo& G, float h2, int k, int own_lo, int own_hi, int held
   return PDE_OK;
 }
 
-void launch_jacobi(const JacobiLaunch& L, cudaStream_t st, const float* pin, float* pout, const float* rhs,
-                   float* resid, const J2Params& JP, const PdeBCRules& R) {
+int launch_jacobi(const JacobiLaunch& L, cudaStream_t st, const float* pin, float* pout, const float* rhs,
+                  float* resid, const J2Params& JP, const PdeBCRules& R) {
   switch (L.cpt) {
-    case 4: jacobi2d_cells_kernel<4><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
-    case 6: jacobi2d_cells_kernel<6><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
-    case 8: jacobi2d_cells_kernel<8><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
-    case 12: jacobi2d_cells_kernel<12><<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
-    default: jacobi2d_tb_kernel<<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R); break;
+    case 4: return launch_pdl(jacobi2d_cells_kernel<4>, L.tiles, L.threads, L.smem, st, pin, pout, rhs, resid, JP, R);
+    case 6: return launch_pdl(jacobi2d_cells_kernel<6>, L.tiles, L.threads, L.smem, st, pin, pout, rhs, resid, JP, R);
+    case 8: return launch_pdl(jacobi2d_cells_kernel<8>, L.tiles, L.threads, L.smem, st, pin, pout, rhs, resid, JP, R);
+    case 12:
+      return launch_pdl(jacobi2d_cells_kernel<12>, L.tiles, L.threads, L.smem, st, pin, pout, rhs, resid, JP, R);
+    default:
+      jacobi2d_tb_kernel<<<L.tiles, L.threads, L.smem, st>>>(pin, pout, rhs, resid, JP, R);
+      return launch_status();
   }
 }
 
@@ -1156,7 +1178,8 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
       JP.k = (iters - done < k) ? (iters - done) : k;
       done += JP.k;
       JP.last = (done == iters);
-      launch_jacobi(JL, st, src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
+      rc = launch_jacobi(JL, st, src, dst, rhs, resid ? resid + step : nullptr, JP, *p_rules);
+      if (rc) return rc;
       float* t = src;
       src = dst;
       dst = t;
@@ -1299,7 +1322,8 @@ int pde_ldc_slab_step(int32_t phase, float* u, float* u_star, const float* p_in,
       if (rc) return rc;
       JP.k = nsweeps;
       JP.last = last ? 1 : 0;
-      launch_jacobi(JL, st, gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1), resid, JP, *p_rules);
+      rc = launch_jacobi(JL, st, gl(p_in, 1), const_cast<float*>(gl(p_out, 1)), gl(rhs, 1), resid, JP, *p_rules);
+      if (rc) return rc;
       break;
     }
     default:
