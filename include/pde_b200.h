@@ -217,7 +217,10 @@ int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* gri
  * u_in: initial field; u_out: result; work: scratch of the same size (used as the
  * ping-pong buffer when nsteps > steps_per_pass).  u_out may equal u_in.
  * steps_per_pass: temporal-blocking depth k (0 = choose).  2D (Z == 1) grids use
- * shared-memory tiles with k steps per pass; 3D grids use k = 1.
+ * shared-memory tiles with k steps per pass.  3D grids whose interior has at
+ * least 3 cells per axis stream along X with k steps per pass (k at most 4 for
+ * one component, 2 for more; deeper requests run at that depth); smaller 3D
+ * grids take one step per pass.
  * Constant-valued groups only: rules with a ramp group (has_ramp) give
  * PDE_ERR_UNSUPPORTED here; pde_heat_rollout_at takes them. */
 int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
@@ -382,6 +385,14 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
  * cells per thread runs the register cell-list Jacobi kernel, others the
  * flat-walk kernel (same results). */
 int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads);
+
+/* Launch shape of the 3D streaming heat rollout (pde_heat_rollout[_at] on 3D
+ * grids): largest tile sides along Y and Z (capped at the compiled maxima, 32
+ * for one component) and the number of chunks the X axis is split into
+ * (items = tiles x chunks on a persistent grid); 0 = chosen per launch.
+ * Process-wide; for tuning.  Results do not depend on it.  No counterpart in
+ * the reference (its kernels are launched by Warp). */
+int pde_set_launch_3d(int32_t tile_y, int32_t tile_z, int32_t chunks);
 
 /* ---- batched rollouts (new: the reference advances every grid with its own
  * module chain, examples/2D_Heat_Equation.py:57-65, three launches per step

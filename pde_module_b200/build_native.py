@@ -18,11 +18,11 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_native")
 LIB = os.path.join(OUT_DIR, "libpde_b200.so")
 
-SOURCES = ["pde_b200.cu", "noalloc.cu", "immersed.cu", "acm.cu"]
+SOURCES = ["pde_b200.cu", "heat3d.cu", "noalloc.cu", "immersed.cu", "acm.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr",
 ]
 
@@ -41,21 +41,40 @@ def _newest_source_mtime() -> float:
 
 
 def build(force: bool = False, verbose: bool = False, extra_flags: list[str] | None = None) -> str:
-    """Compile the library if missing or older than its sources; return its path."""
+    """Compile the library if missing or older than its sources; return its path.
+
+    Each source compiles to an object in its own nvcc process (in parallel),
+    then nvcc links the shared library."""
     os.makedirs(OUT_DIR, exist_ok=True)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_source_mtime():
         return LIB
-    cmd = [nvcc_path(), *NVCC_FLAGS, *(extra_flags or []),
-           "-I", os.path.join(ROOT, "include"),
-           *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp"]
-    if verbose:
-        print(" ".join(cmd), flush=True)
+    nvcc = nvcc_path()
+    obj_dir = os.path.join(OUT_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    jobs = []
+    for src in SOURCES:
+        obj = os.path.join(obj_dir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc, *NVCC_FLAGS, *(extra_flags or []), "-I", os.path.join(ROOT, "include"),
+               "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        jobs.append((obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)))
+    failed = False
+    for obj, proc in jobs:
+        out, _ = proc.communicate()
+        if proc.returncode != 0:
+            failed = True
+            sys.stderr.write(out)
+        elif verbose and out:
+            sys.stderr.write(out)
+    if failed:
+        raise RuntimeError("nvcc failed building libpde_b200.so")
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC",
+           *[o for o, _ in jobs], "-o", LIB + ".tmp"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
-        raise RuntimeError("nvcc failed building libpde_b200.so")
-    if verbose and (res.stdout or res.stderr):
-        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("nvcc failed linking libpde_b200.so")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

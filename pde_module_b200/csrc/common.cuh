@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <type_traits>
+
 #include "../../include/pde_b200.h"
 
 namespace pde {
@@ -152,6 +154,51 @@ __device__ __forceinline__ f2 mul2(f2 a, f2 b) {
   f2 d;
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
   return d;
+}
+
+// Boundary time of rollout step n: t0 + n * tstep in double, each operation
+// rounded on its own (as a host caller computes t0 + n*dt), then rounded to fp32.
+__device__ __forceinline__ float step_time(double t0, double tstep, int n) {
+  return __double2float_rn(__dadd_rn(t0, __dmul_rn((double)n, tstep)));
+}
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I = I0 .. N-1.
+template <int I, int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+  if constexpr (I < N) {
+    f(std::integral_constant<int, I>{});
+    static_for<I + 1, N>(f);
+  }
+}
+
+// SMs of the current device (looked up once per process).
+inline int sm_count() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+      n = 148;
+  }
+  return n;
+}
+
+// Launch with programmatic stream serialization: the kernel may be scheduled
+// while the previous kernel of the stream runs; it calls pdl_wait before any
+// global access to data another launch reads or writes.
+template <typename... KArgs, typename... Args>
+int launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...) == cudaSuccess ? PDE_OK : PDE_ERR_CUDA;
 }
 
 inline int grid_blocks(int64_t work, int threads, int64_t cap = 148LL * 64) {

@@ -147,11 +147,6 @@ struct H2Params {
   int n0;
 };
 
-// Boundary time of rollout step n: t0 + n * tstep in double, each operation
-// rounded on its own (as a host caller computes t0 + n*dt), then rounded to fp32.
-__device__ __forceinline__ float step_time(double t0, double tstep, int n) {
-  return __double2float_rn(__dadd_rn(t0, __dmul_rn((double)n, tstep)));
-}
 
 // Boundary fill of the smem region (array rectangle [rx0,rx0+RX) x [ry0,ry0+RY)),
 // in place: ghosts first (they read pre-boundary interior values), then nodes.

@@ -21,16 +21,6 @@ namespace {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-int sm_count() {
-  static int n = 0;
-  if (n == 0) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
-      n = 148;
-  }
-  return n;
-}
 
 int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ERR_CUDA; }
 
@@ -42,23 +32,6 @@ int g_threads2d = 0;
 // A 2D tile count just above m x SMs (m = 1, 2) leaves a short tail wave in which
 // a few SMs run a second tile while the rest wait: enlarge the tiles slightly
 // (at most two fewer tiles per axis, sides up to 256) so the count drops to m x SMs.
-// Launch with programmatic stream serialization: the kernel may be scheduled
-// while the previous kernel of the stream runs; it calls pdl_wait before any
-// global access to data another launch reads or writes.
-template <typename... KArgs, typename... Args>
-int launch_pdl(void (*kern)(KArgs...), int grid, int block, size_t smem, cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
-  cfg.blockDim = dim3((unsigned)block);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kern, args...) == cudaSuccess ? PDE_OK : PDE_ERR_CUDA;
-}
 
 void balance_tiles(int X, int Y, int* tbx, int* tby) {
   const long long sms = sm_count();
@@ -501,7 +474,26 @@ int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* gri
   return PDE_OK;
 }
 
+// 3D streaming heat rollout (heat3d.cu)
+extern "C++" {
+namespace pde {
+int heat3d_kmax(int ncomp);
+int launch_heat3d(int ks, int R, int N, const float* src, float* dst, const Geo& G, const Weights& W, float alpha,
+                  float dt, const PdeBCRules* rules, double t0, double tstep, int n0, cudaStream_t st);
+}  // namespace pde
+}
+
 namespace {
+
+// The streaming kernel takes 3D grids whose interior has at least 3 cells per
+// axis, and whose planes index in 32 bits.
+bool heat3d_ok(const Geo& G, int ncomp) {
+  if (g_dispatch == PDE_DISPATCH_GENERIC) return false;
+  if (G.ndims != 3 || ncomp < 1 || ncomp > 4) return false;
+  for (int a = 0; a < 3; ++a)
+    if (G.ext[a] < 3) return false;
+  return G.n[1] * G.n[2] * ncomp < (1LL << 31);
+}
 
 // Host copy of generic.cuh bc_value for a ramp group at rollout step n: the
 // same float operations (t / t_max rounded, min with 1, times the value).
@@ -534,7 +526,12 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
   const Weights W = lap_weights(G.order, grid->dx);
   const int R = W.radius;
   const bool two_d = (G.ndims == 2 && G.n[2] == 1);
+  const bool s3d = !two_d && heat3d_ok(G, ncomp);
   int k = two_d ? (steps_per_pass > 0 ? steps_per_pass : 8) : 1;
+  if (s3d) {
+    k = steps_per_pass > 0 ? steps_per_pass : 2;
+    if (k > heat3d_kmax(ncomp)) k = heat3d_kmax(ncomp);
+  }
   if (k > nsteps) k = nsteps;
   const int npasses = (nsteps + k - 1) / k;
   // buffer sequence: the last pass writes u_out.
@@ -623,6 +620,9 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
       }
 #undef PDE_H2
       }
+    } else if (s3d) {
+      const int lrc = launch_heat3d(ks, R, ncomp, src, dst, G, W, alpha, dt, rules, t0, tstep, done, st);
+      if (lrc) return lrc;
     } else {
       const int64_t total = G.n[0] * G.n[1] * G.n[2] * ncomp;
       // one step per launch: time-dependent group values are set in a copy of the rules

@@ -39,14 +39,6 @@ struct S3Params {
 
 __host__ __device__ constexpr int round4(int v) { return (v + 3) & ~3; }
 
-template <int I, int N, class F>
-__device__ __forceinline__ void static_for(F&& f) {
-  if constexpr (I < N) {
-    f(std::integral_constant<int, I>{});
-    static_for<I + 1, N>(f);
-  }
-}
-
 // Plane addressing: MAP_ROWS_GEN / MAP_ROWS_PP0 bring each tile row with its
 // own 1D TMA copy (the lead of a row inside its 16-byte aligned copy varies
 // with the plane in the GEN case, is fixed in the PP0 case); MAP_PAIRS views

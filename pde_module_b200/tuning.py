@@ -69,6 +69,13 @@ def tune_stream3d(interior=(512, 512, 512), orders=(2, 4), reps: int = 5, kinds=
     return out
 
 
+def set_launch_3d(tile_y: int = 0, tile_z: int = 0, chunks: int = 0) -> None:
+    """Launch shape of the 3D streaming heat rollout: tile sides along Y and Z
+    (capped at the compiled maxima) and the number of X chunks; 0 = automatic.
+    Results do not depend on it."""
+    _lib.check(_lib.lib().pde_set_launch_3d(int(tile_y), int(tile_z), int(chunks)), "pde_set_launch_3d")
+
+
 def tune_heat_depth(rollout, u: torch.Tensor, nsteps: int = 256, depths=(1, 2, 4, 8, 16), reps: int = 3) -> int:
     """Set rollout.steps_per_pass to the fastest temporal-blocking depth for field u."""
     best, best_ms = None, None
