@@ -36,9 +36,9 @@ int launch_heat3d_k(const float* src, float* dst, const Geo& G, const Weights& W
   P.nz_t = (P.Z + tz - 1) / tz;
   P.ntiles = P.ny_t * P.nz_t;
   // X chunks (balanced, each at least min_chunk planes, which the ghost planes
-  // at either end of X need): the kernel is bound by instruction issue, so the
-  // busiest SM runs ceil(items / SMs) items of about X/n + 2H planes each (an
-  // item streams H extra planes at either end), whatever number share the SM.
+  // at either end of X need).  The kernel is bound by instruction issue and
+  // the items are dealt evenly, so the time is about the total planes streamed
+  // (each item streams 2H extra) over the SMs, plus one item of granularity.
   const int H = Cf::H;
   const long long sms = sm_count();
   const long long slots = (long long)occ * sms;
@@ -50,8 +50,8 @@ int launch_heat3d_k(const float* src, float* dst, const Geo& G, const Weights& W
   } else {
     double best = 1e300;
     for (int n = 1; n <= max_n; ++n) {
-      const long long items = (long long)P.ntiles * n;
-      const double cost = (double)((items + sms - 1) / sms) * ((double)P.X / n + 2 * H);
+      const double per_item = (double)P.X / n + 2 * H;
+      const double cost = (double)P.ntiles * n * per_item / (double)sms + per_item;
       if (cost < best - 1e-9) { best = cost; best_n = n; }
     }
   }
@@ -74,35 +74,37 @@ int launch_heat3d(int ks, int R, int N, const float* src, float* dst, const Geo&
                   float dt, const PdeBCRules* rules, double t0, double tstep, int n0, cudaStream_t st) {
 #define PDE_H3(RR, KK, NN, TY, TZ, TT) \
   return launch_heat3d_k<RR, KK, NN, TY, TZ, TT>(src, dst, G, W, alpha, dt, rules, t0, tstep, n0, st)
+  // tile shapes: the region (tile + 2H per axis, rows rounded to 8, row pitch
+  // to 8 floats) fills whole warp tiles of T/32 warps; registers bound T * C
   if (N == 1) {
     if (R == 1) {
       switch (ks) {
-        case 1: PDE_H3(1, 1, 1, 32, 32, 256);
-        case 2: PDE_H3(1, 2, 1, 32, 32, 256);
-        case 3: PDE_H3(1, 3, 1, 32, 32, 512);
-        default: PDE_H3(1, 4, 1, 32, 32, 512);
+        case 1: PDE_H3(1, 1, 1, 44, 26, 256);
+        case 2: PDE_H3(1, 2, 1, 42, 24, 256);
+        case 3: PDE_H3(1, 3, 1, 40, 22, 384);
+        default: PDE_H3(1, 4, 1, 38, 28, 480);
       }
     }
     switch (ks) {
-      case 1: PDE_H3(2, 1, 1, 32, 32, 256);
-      case 2: PDE_H3(2, 2, 1, 32, 32, 512);
-      case 3: PDE_H3(2, 3, 1, 24, 24, 512);
-      default: PDE_H3(2, 4, 1, 16, 16, 512);
+      case 1: PDE_H3(2, 1, 1, 42, 24, 256);
+      case 2: PDE_H3(2, 2, 1, 38, 28, 480);
+      case 3: PDE_H3(2, 3, 1, 18, 16, 512);
+      default: PDE_H3(2, 4, 1, 14, 12, 512);
     }
   }
   if (N == 2) {
-    if (R == 1) { if (ks == 1) PDE_H3(1, 1, 2, 32, 16, 256); PDE_H3(1, 2, 2, 32, 16, 256); }
-    if (ks == 1) PDE_H3(2, 1, 2, 32, 16, 256);
-    PDE_H3(2, 2, 2, 32, 16, 512);
+    if (R == 1) { if (ks == 1) PDE_H3(1, 1, 2, 44, 11, 256); PDE_H3(1, 2, 2, 42, 9, 256); }
+    if (ks == 1) PDE_H3(2, 1, 2, 42, 9, 256);
+    PDE_H3(2, 2, 2, 38, 9, 480);
   }
   if (N == 3) {
-    if (R == 1) { if (ks == 1) PDE_H3(1, 1, 3, 32, 12, 512); PDE_H3(1, 2, 3, 32, 12, 512); }
-    if (ks == 1) PDE_H3(2, 1, 3, 32, 12, 512);
-    PDE_H3(2, 2, 3, 32, 12, 512);
+    if (R == 1) { if (ks == 1) PDE_H3(1, 1, 3, 44, 6, 256); PDE_H3(1, 2, 3, 42, 6, 480); }
+    if (ks == 1) PDE_H3(2, 1, 3, 42, 6, 480);
+    PDE_H3(2, 2, 3, 38, 5, 384);
   }
-  if (R == 1) { if (ks == 1) PDE_H3(1, 1, 4, 32, 8, 512); PDE_H3(1, 2, 4, 32, 8, 512); }
-  if (ks == 1) PDE_H3(2, 1, 4, 32, 8, 512);
-  PDE_H3(2, 2, 4, 32, 6, 512);
+  if (R == 1) { if (ks == 1) PDE_H3(1, 1, 4, 44, 3, 256); PDE_H3(1, 2, 4, 42, 3, 480); }
+  if (ks == 1) PDE_H3(2, 1, 4, 42, 3, 480);
+  PDE_H3(2, 2, 4, 38, 3, 448);
 #undef PDE_H3
 }
 

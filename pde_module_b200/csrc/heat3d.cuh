@@ -15,8 +15,10 @@
 // region (the tile, at level K): what they read was valid at level s-1.
 //
 // Storage.  A region row is stored from an even float (the row's first cell
-// rounded down), so a plane is a sequence of float pairs; thread t owns pairs
-// t + c*T.  Per level each thread keeps its pairs' boundary-filled values for
+// rounded down), so a plane is a sequence of float pairs.  Pairs are dealt to
+// warps in "warp tiles" of 8 rows x 4 pairs (lane = 4 * row + pair), warp w
+// taking tiles w + c*W: cells at the array's boundary then fall into a few
+// warps, and the rest run a path with no boundary test.  Per level each thread keeps its pairs' boundary-filled values for
 // the last 2R+1 planes in registers (X taps, a queue rotated each plane).  Y and
 // Z taps come from the plane of the level below in shared memory: level 0's
 // plane is the cp.async staging slot (4-byte copies: any row pitch), levels
@@ -71,12 +73,14 @@ template <int R, int K, int N, int TYM, int TZM, int T>
 struct H3Cfg {
   static constexpr int H = K * R + 1;                     // region halo
   static constexpr int RYM = TYM + 2 * H;                 // region rows (max)
-  static constexpr int P = ((TZM + 2 * H) * N + 2) & ~1;  // row pitch (floats): row + even-start lead, even
-  static constexpr int PLANE = RYM * P;
-  static constexpr int NPR = PLANE / 2;                   // pairs per plane
-  static constexpr int C = (NPR + T - 1) / T;             // pairs per thread
+  static constexpr int P = ((TZM + 2 * H) * N + 2 + 7) & ~7;  // row pitch (floats): row + even-start lead
+  static constexpr int W = T / 32;                        // warps
+  static constexpr int NWC = P / 8, NWR = (RYM + 7) / 8;  // warp tiles (8 rows x 8 floats) per row / column
+  static constexpr int NWT = NWR * NWC;
+  static constexpr int C = (NWT + W - 1) / W;             // pairs per thread (warp tiles per warp)
+  static constexpr int PLANE = NWR * 8 * P;               // floats of a plane (rows rounded up to 8)
   static constexpr int G0 = R * P;                        // guard floats before a plane's first row
-  static constexpr int PS = (2 * R * P + 2 * C * T + 3) & ~3;  // plane slot stride (floats)
+  static constexpr int PS = (PLANE + 2 * R * P + 3) & ~3;  // plane slot stride (floats)
   static constexpr int PF = 3;                            // planes in flight ahead of level 0
   static constexpr int S = PF + R + 1;                    // staging slots
   static constexpr int NB = (K - 1) * (R + 1);            // ring planes of levels 1..K-1
@@ -86,6 +90,7 @@ struct H3Cfg {
   static constexpr size_t SMEM = (size_t)NPL * PS * 4 + (size_t)3 * PLANE * 4 + sizeof(PdeBCRules) +
                                  (size_t)K * PDE_MAX_GROUPS * 4;
   static_assert(2 * C <= 32, "lane masks");
+  static_assert(T % 32 == 0, "whole warps");
   static_assert(SMEM <= 227 * 1024, "shared memory per block");
   static_assert(K >= 1 && K <= 4, "steps per pass");
 };
@@ -222,11 +227,43 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
   const float2 al2 = make_float2(P.alpha, P.alpha), dt2 = make_float2(P.dt, P.dt),
                nz2 = make_float2(P.negzero, P.negzero);
 
+  // float offset in a plane of each of this thread's pairs (PLANE: past the
+  // plane, for the slots of warp tiles beyond the last)
+  int rc[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int wt = (tid >> 5) + c * Cf::W, lane = tid & 31;
+    const int wr = wt / Cf::NWC, wc = wt - wr * Cf::NWC;
+    rc[c] = wt < Cf::NWT ? (wr * 8 + (lane >> 2)) * PP + 2 * (wc * 4 + (lane & 3)) : PL;
+  }
+
   pdl_wait();
 
-  for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
-    const int ch = item / P.ntiles, tile = item - ch * P.ntiles;
-    const int ty = tile / P.nz_t, tz = tile - ty * P.nz_t;
+  // Work items in order of cost: tiles at the Y/Z edges of the array (boundary
+  // work) first, then the others, chunk-major within each class; round k of
+  // the persistent grid deals items k*G .. k*G+G-1 to the blocks forward on
+  // even rounds and backward on odd ones, so every block gets a like share.
+  const int G = gridDim.x, nyt = P.ny_t, nzt = P.nz_t;
+  const bool all_edge = nyt <= 2 || nzt <= 2;
+  const int ne = all_edge ? P.ntiles : 2 * nzt + 2 * (nyt - 2), ni = P.ntiles - ne;
+  for (int kr = 0;; ++kr) {
+    const int item = kr * G + ((kr & 1) ? G - 1 - (int)blockIdx.x : (int)blockIdx.x);
+    if (item >= P.nitems) break;
+    int ch, ty, tz;
+    if (item < ne * P.nch) {
+      ch = item / ne;
+      const int e = item - ch * ne;
+      if (all_edge) { ty = e / nzt; tz = e - ty * nzt; }
+      else if (e < nzt) { ty = 0; tz = e; }
+      else if (e < 2 * nzt) { ty = nyt - 1; tz = e - nzt; }
+      else { const int m = e - 2 * nzt; ty = 1 + (m >> 1); tz = (m & 1) ? nzt - 1 : 0; }
+    } else {
+      const int j = item - ne * P.nch;
+      ch = j / ni;
+      const int t2 = j - ch * ni;
+      ty = 1 + t2 / (nzt - 2);
+      tz = 1 + t2 % (nzt - 2);
+    }
     const int y0 = (int)((long long)ty * Y / P.ny_t), y1 = (int)((long long)(ty + 1) * Y / P.ny_t);
     const int z0 = (int)((long long)tz * Z / P.nz_t), z1 = (int)((long long)(tz + 1) * Z / P.nz_t);
     const int ya = max(0, y0 - H), yb = min(Y, y1 + H);
@@ -241,19 +278,25 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
     // lane masks (bit 2c+l: lane l of pair c): active per level, fast (no boundary
     // work on planes g+2..X-g-3), first-layer Y/Z ghost column, stencil column
     uint32_t am[K + 1], fm = 0, gm = 0, scm = 0;
+    uint32_t wtm = 0;  // bit c: pair c's warp tile holds region cells (the same in every lane of a warp)
 #pragma unroll
     for (int s = 0; s <= K; ++s) am[s] = 0;
     int goff[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      const int r = 2 * (tid + c * T);
+      const int r = rc[c];
       const int ry = r / PP, rz = r - ry * PP;
+      {
+        const int wt = (tid >> 5) + c * Cf::W;
+        const int wr = wt / Cf::NWC, wc = wt - wr * Cf::NWC;
+        if (wt < Cf::NWT && ya + wr * 8 < yb && zr0 + wc * 8 < zhi) wtm |= 1u << c;
+      }
       const int y = ya + ry;
       goff[c] = y * ZN + zr0 + rz;
 #pragma unroll
       for (int l = 0; l < 2; ++l) {
         const int zv = zr0 + rz + l;
-        if (y >= yb || zv < zlo || zv >= zhi) continue;
+        if (r >= PL || y >= yb || zv < zlo || zv >= zhi) continue;
         const int z = zv / N;
         int d = 1 << 20;
         if (ya > 0) d = min(d, y - ya);
@@ -278,6 +321,8 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
       }
     }
 
+    const bool allw = wtm == (1u << C) - 1u;  // every warp tile of this warp live: loops without per-pair tests
+
     // level-0 staging: plane p lives in slot (p - xa) % S; lanes outside the
     // region are zero filled without a read
     auto issue = [&](int p, int slot) {
@@ -285,8 +330,8 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
         float* dst = stage + slot * PS;
         const float* src = in + (long long)p * YZN;
 #pragma unroll
-        for (int c = 0; c < C; ++c) {
-          const int r = 2 * (tid + c * T);
+        for (int c = 0; c < C; ++c) {  // dead warp tiles: zero fill past the plane, no read
+          const int r = rc[c];
           const bool v0 = (am[0] >> (2 * c)) & 1u, v1 = (am[0] >> (2 * c + 1)) & 1u;
           cp_async4(dst + r, v0 ? src + goff[c] : in, v0);
           cp_async4(dst + r + 1, v1 ? src + goff[c] + 1 : in, v1);
@@ -336,7 +381,7 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
     // boundary fill of lane l of pair c at level s, plane x, pre-boundary value u
     // (level 0: read here from Bs unless another thread writes the cell)
     auto fill = [&](int s, int x, int c, int l, float u, bool level0, float* Bs, float2 (&qs)[Q]) {
-      const int rr = 2 * (tid + c * T) + l;
+      const int rr = rc[c] + l;
       const float* gv = gval + s * PDE_MAX_GROUPS;
       if (x >= g && x <= X - 1 - g) {
         const int cx = x == g ? 0 : (x == X - 1 - g ? 2 : 1);
@@ -377,8 +422,14 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
         const bool inx = i >= g + 2 && i <= X - g - 3;
         const uint32_t gen = inx ? ((am[0] & ~fm) | gm) : am[0];  // lanes with boundary work
 #pragma unroll
-        for (int c = 0; c < C; ++c)
-          if (!((gm >> (2 * c)) & 3u)) q[0][c][0] = *reinterpret_cast<const float2*>(St + 2 * (tid + c * T));
+        if (allw && !gm) {
+#pragma unroll
+          for (int c = 0; c < C; ++c) q[0][c][0] = *reinterpret_cast<const float2*>(St + rc[c]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < C; ++c)
+            if (((wtm >> c) & 1u) && !((gm >> (2 * c)) & 3u)) q[0][c][0] = *reinterpret_cast<const float2*>(St + rc[c]);
+        }
         if (gen) {
 #pragma unroll
           for (int c = 0; c < C; ++c)
@@ -404,17 +455,28 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
         const uint32_t gen = inx ? ((am[s] & ~fm) | gm) : am[s];
         if (!gen) {  // no boundary work in this thread's pairs
 #pragma unroll
-          for (int c = 0; c < C; ++c) {
-            const int r = 2 * (tid + c * T);
-            const float2 u = core(q[s - 1][c], Bp, r, q[s - 1][c][R]);
-            q[s][c][0] = u;
-            *reinterpret_cast<float2*>(Bs + r) = u;
+          if (allw) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+              const float2 u = core(q[s - 1][c], Bp, rc[c], q[s - 1][c][R]);
+              q[s][c][0] = u;
+              *reinterpret_cast<float2*>(Bs + rc[c]) = u;
+            }
+          } else {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+              if (!((wtm >> c) & 1u)) continue;
+              const float2 u = core(q[s - 1][c], Bp, rc[c], q[s - 1][c][R]);
+              q[s][c][0] = u;
+              *reinterpret_cast<float2*>(Bs + rc[c]) = u;
+            }
           }
           return;
         }
 #pragma unroll
         for (int c = 0; c < C; ++c) {
-          const int r = 2 * (tid + c * T);
+          if (!((wtm >> c) & 1u)) continue;
+          const int r = rc[c];
           if (!((gen >> (2 * c)) & 3u)) {
             const float2 u = core(q[s - 1][c], Bp, r, q[s - 1][c][R]);
             q[s][c][0] = u;
@@ -442,15 +504,25 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
           float* orow = out + (long long)x * YZN;
           if (inx && !gm && !(am[K] & ~fm)) {  // every output lane a stencil cell
 #pragma unroll
+            float2 u[C];
+            if (allw) {
+#pragma unroll
+              for (int c = 0; c < C; ++c) u[c] = core(q[K - 1][c], Bp, rc[c], q[K - 1][c][R]);
+            } else {
+#pragma unroll
+              for (int c = 0; c < C; ++c)
+                if ((wtm >> c) & 1u) u[c] = core(q[K - 1][c], Bp, rc[c], q[K - 1][c][R]);
+            }
+#pragma unroll
             for (int c = 0; c < C; ++c) {
-              const float2 u = core(q[K - 1][c], Bp, 2 * (tid + c * T), q[K - 1][c][R]);
-              if ((am[K] >> (2 * c)) & 1u) orow[goff[c]] = u.x;
-              if ((am[K] >> (2 * c + 1)) & 1u) orow[goff[c] + 1] = u.y;
+              if ((am[K] >> (2 * c)) & 1u) orow[goff[c]] = u[c].x;
+              if ((am[K] >> (2 * c + 1)) & 1u) orow[goff[c] + 1] = u[c].y;
             }
           } else {
 #pragma unroll
             for (int c = 0; c < C; ++c) {
-              const float2 u = step(q[K - 1][c], Bp, 2 * (tid + c * T), c, xst);
+              if (!((wtm >> c) & 1u)) continue;
+              const float2 u = step(q[K - 1][c], Bp, rc[c], c, xst);
               if ((am[K] >> (2 * c)) & 1u) orow[goff[c]] = u.x;
               if ((am[K] >> (2 * c + 1)) & 1u) orow[goff[c] + 1] = u.y;
             }
