@@ -35,6 +35,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_INT = 512
+# interior side of the CPU sample of the sweep (both arms time the same sample)
+CPU_SAMPLE_N = 128
 METRIC = "cell-updates/s (3D operator sweep: Laplacian, Grad, Divergence; order 2 and 4)"
 UNIT = "cell-updates/s"
 # algorithmic bytes per interior cell: compulsory read once + write once
@@ -225,7 +227,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    n = 96
+    n = CPU_SAMPLE_N
     for _ in range(args.warmup):
         cpu_sweep_sample(n, threads)
     vals = []
@@ -239,7 +241,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_all / max(args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": sweep_config(args.gpus),
+        "config": dict(sweep_config(args.gpus), cpu_sample_interior=[n, n, n]),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"each step: the 6-operator step on a {n}^3 interior (order 2 and 4), NumPy "
                                    f"float32 restatement of the reference kernels (the reference's own code needs "
@@ -405,6 +407,9 @@ def run_ours(args):
     if not args.no_e2e:
         e2e = run_e2e(fields, ops, world, args)
 
+    heat3d = None
+    if world == 1 and not args.no_heat3d:  # a single-GPU workload (replicas only): not run beside other ranks
+        heat3d = run_heat3d()
     heat = None
     if world == 1 and not args.no_heat:  # a single-GPU workload (replicas only): not run beside other ranks
         heat = run_heat()
@@ -430,9 +435,9 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
-        v, dt = cpu_sweep_sample(128, threads, min_seconds=10.0)
+        v, dt = cpu_sweep_sample(CPU_SAMPLE_N, threads, min_seconds=10.0)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"the 6-operator step on a 128^3 interior repeated for {dt:.1f} s, NumPy float32 "
+               "sample": f"the 6-operator step on a {CPU_SAMPLE_N}^3 interior repeated for {dt:.1f} s, NumPy float32 "
                          f"restatement of the reference kernels (oracle/fdm.py), X slabs over {threads} threads"}
 
     if rank == 0:
@@ -453,8 +458,10 @@ def run_ours(args):
             "batched_64": batched,
             "wc_cavity": wc,
             "autotune": {f"{k[0]}_n{k[1]}_o{k[2]}": v for k, v in tuned.items()},
+            "heat3d_512": heat3d,
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": K * len(ops), "clocks": clocks,
+            "summary": leg_summary(kern, heat3d, heat, ldc, wave, batched, wc),
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -465,6 +472,112 @@ def run_ours(args):
 
 # launch shapes (tile_x, tile_y, threads) tried for the temporally blocked 2D kernels (0: automatic)
 TILES_2D = ((0, 0, 0), (32, 64, 1024), (32, 64, 512), (32, 32, 512), (32, 32, 256), (16, 32, 256), (16, 64, 256))
+
+
+def heat256_initial(n: int = 256, g: int = 1) -> np.ndarray:
+    """The 2D heat workload's initial field: U[0,1) from seed 0 on the n x n
+    interior times a Gaussian bump of sigma 0.1 centred at (0.5, 0.5), with
+    node-centred coordinates x_i = i/n (mesh/uniformGridMesh/functions.py:81-84);
+    ghost cells 0.  Shape (n+2g, n+2g, 1, 1), float32."""
+    rng = np.random.default_rng(0)
+    x = np.arange(n) / n
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    u = np.zeros((n + 2 * g, n + 2 * g, 1, 1), dtype=np.float32)
+    u[g:n + g, g:n + g, 0, 0] = (rng.random((n, n)) *
+                                 np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / (2 * 0.1 ** 2))).astype(np.float32)
+    return u
+
+
+def run_heat3d(n: int = 512, steps: int = 12, depths=(1, 2, 3, 4)):
+    """3D heat, n^3 interior + 1 ghost (order 2) or 2 (order 4), Dirichlet 0 on
+    every face, alpha 1, dt = 0.15 dx^2, u0 = U[0,1) (seeded): the fused 3D
+    rollout (boundary fill + Laplacian + Euler streamed along X, k steps per HBM
+    pass) at each depth k, CUDA events around `steps` steps (best of 3), and a
+    bitwise check of the fastest depth against the one-step-per-launch kernel.
+    Fields (0.54 GB each) are larger than L2."""
+    import torch
+    import pde_module_b200 as P
+    from pde_module_b200 import _lib
+    peak, peak_kind = peaks()
+    out = {"workload": f"3D heat {n}^3, Dirichlet 0 on all faces, alpha 1, dt 0.15 dx^2 (the heat loop of "
+                       "examples/2D_Heat_Equation.py on a 3D grid), exact arithmetic"}
+    for order in (2, 4):
+        g = order // 2
+        s = n + 2 * g
+        dx = 1.0 / (n - 1)
+        gen = torch.Generator(device="cuda")
+        gen.manual_seed(11)
+        u = torch.rand((s, s, s, 1), device="cuda", generator=gen)
+        bc = P.GridBoundary(u, dx, g)
+        bc.dirichlet_BC("ALL", 0.0)
+        dt = 0.15 * dx * dx
+        res = {}
+        for k in depths:
+            roll = P.HeatRollout(bc, dx, 1.0, dt, order=order, steps_per_pass=k)
+            roll(u, steps)
+            torch.cuda.synchronize()
+            best = None
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                roll(u, steps)
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / steps
+                best = t if best is None else min(best, t)
+            cps = n ** 3 / (best / 1000.0)
+            gbs = cps * 8.0 / k / 1e9
+            res[k] = {"ms_per_step": round(best, 4), "cell_updates_per_s": cps,
+                      "alg_bytes_per_cell_step": round(8.0 / k, 3), "alg_gbs": round(gbs, 1),
+                      "frac_of_hbm": round(gbs / peak, 4)}
+        kb = min(res, key=lambda q: res[q]["ms_per_step"])
+        roll = P.HeatRollout(bc, dx, 1.0, dt, order=order, steps_per_pass=kb)
+        fused = roll(u, 4).clone()
+        prev = _lib.lib().pde_set_dispatch(1)
+        single = P.HeatRollout(bc, dx, 1.0, dt, order=order)(u, 4).clone()
+        _lib.lib().pde_set_dispatch(prev)
+        torch.cuda.synchronize()
+        out[f"order{order}"] = {"best_k": kb, "ms_per_step": res[kb]["ms_per_step"],
+                                "cell_updates_per_s": res[kb]["cell_updates_per_s"],
+                                "bitwise_equal_to_single_step_kernel": bool(torch.equal(fused, single)),
+                                "by_k": {f"k{k}": v for k, v in res.items()}}
+        del u, fused, single
+    out["note"] = (f"alg_gbs = 8 B per cell and pass / (ms per step x k), of the {peak_kind} HBM peak {peak} GB/s; "
+                   "the kernel is bound by instruction issue and shared-memory latency (exact arithmetic), not HBM")
+    return out
+
+
+def leg_summary(kern, heat3d, heat, ldc, wave, batched, wc) -> dict:
+    """The key figure of every leg, short (the line's last key)."""
+    def g(d, *path):
+        for p in path:
+            if not isinstance(d, dict) or p not in d:
+                return None
+            d = d[p]
+        return round(d, 4) if isinstance(d, float) else d
+    out = {"sweep_frac": {k: v["frac"] for k, v in kern.items()}}
+    if heat3d:
+        out["heat3d_512"] = {f"o{o}": {"k": g(heat3d, f"order{o}", "best_k"),
+                                       "ms_per_step": g(heat3d, f"order{o}", "ms_per_step"),
+                                       "gcups": round(heat3d[f"order{o}"]["cell_updates_per_s"] / 1e9, 1),
+                                       "bitwise": g(heat3d, f"order{o}", "bitwise_equal_to_single_step_kernel")}
+                             for o in (2, 4)}
+    if heat:
+        out["heat_256"] = {"gcups": round(heat["fused_cell_updates_per_s"] / 1e9, 1),
+                           "x_chain": g(heat, "speedup_vs_chain"),
+                           "fwd_adj_ratio": g(heat, "adjoint", "ratio_fwd_adj_over_fwd")}
+    if wave:
+        out["wave_512"] = {"fwd_ms": g(wave, "forward_ms"), "fwd_adj_ratio": g(wave, "ratio_fwd_adj_over_fwd")}
+    if ldc:
+        out["ldc_1024"] = {"gcups": round(ldc["cell_updates_per_s"] / 1e9, 2),
+                           "jacobi_sweeps_per_s": round(ldc["jacobi_sweeps_per_s"])}
+    if batched:
+        out["batched_64"] = {"heat_x_per_grid_plain": g(batched, "heat", "speedup_vs_plain_chain"),
+                             "heat_x_per_grid_fused": g(batched, "heat", "speedup_vs_per_grid_fused"),
+                             "wave_x_per_grid_fused": g(batched, "wave", "speedup_vs_per_grid_fused")}
+    if wc:
+        out["wc_cavity"] = {"n201_ms": g(wc, "n201", "fused_ms_per_step")}
+    return out
 
 
 def run_heat(steps: int = 1000):
@@ -478,11 +591,7 @@ def run_heat(steps: int = 1000):
     n, g = 256, 1
     dx = 1.0 / n
     dt = 0.2 * dx * dx
-    rng = np.random.default_rng(0)
-    x = (np.arange(n + 2 * g) - g + 0.5) / n
-    X, Y = np.meshgrid(x, x, indexing="ij")
-    u0 = (rng.random((n + 2 * g, n + 2 * g)) * np.exp(-((X - 0.5) ** 2 + (Y - 0.5) ** 2) / (2 * 0.1 ** 2)))
-    u0 = torch.from_numpy(u0.astype(np.float32)[:, :, None, None]).cuda()
+    u0 = torch.from_numpy(heat256_initial(n, g)).cuda()
     bc = P.GridBoundary(u0, dx, g)
     bc.dirichlet_BC("ALL", 0.0)
     lap, euler = P.Laplacian(1, dx, g), P.ForwardEuler()
@@ -1119,6 +1228,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-heat", action="store_true")
+    ap.add_argument("--no-heat3d", action="store_true")
     ap.add_argument("--no-ldc", action="store_true")
     ap.add_argument("--no-wave", action="store_true")
     ap.add_argument("--no-batched", action="store_true")

@@ -119,6 +119,22 @@ const char* pde_strerror(int status);
  * bounds checks that failed).  0 = none.  Synchronises the given stream. */
 int         pde_device_error(void* stream);
 
+/* Bound of every device-side wait of the library (the stream3d kernels'
+ * mbarrier waits, the batched rollout's tile-progress waits): a wait that runs
+ * this long gives up, records PDE_ERR_TIMEOUT in the error word and lets its
+ * kernel return; once the word is set, every other wait gives up at once.
+ * ns = 0 restores the default (2 s).  Process-wide, read at each launch;
+ * returns the previous bound.  No counterpart in the reference (Warp kernels
+ * do not wait on one another). */
+#define PDE_WAIT_LIMIT_DEFAULT_NS 2000000000ull
+uint64_t    pde_set_wait_limit_ns(uint64_t ns);
+
+/* Test hook of the bounded wait: one thread waits until *word >= target (word:
+ * a device uint32) with the progress-wait code of the batched rollout, under
+ * the current bound, and records PDE_ERR_TIMEOUT if it gives up.  No
+ * counterpart in the reference. */
+int         pde_wait_probe(const uint32_t* word, uint32_t target, void* stream);
+
 /* Kernel selection for pde_laplacian/pde_grad/pde_divergence: PDE_DISPATCH_AUTO
  * picks the TMA streaming kernels where they apply, PDE_DISPATCH_GENERIC forces
  * the general kernels (same arithmetic, used to cross-check the two bitwise).

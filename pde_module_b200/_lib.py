@@ -164,6 +164,8 @@ _SIGS = {
                                 C.c_void_p, C.c_int64, C.c_int32, C.c_void_p, C.POINTER(PdeGrid), C.c_void_p]),
     "pde_set_launch_2d": (C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
     "pde_set_launch_3d": (C.c_int, [C.c_int32, C.c_int32, C.c_int32]),
+    "pde_set_wait_limit_ns": (C.c_uint64, [C.c_uint64]),
+    "pde_wait_probe": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p]),
     "pde_heat_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid),
                                    C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_void_p]),

@@ -55,6 +55,7 @@ struct BatchParams {
   int g;
   unsigned int* counter;   // work queue head (zeroed before the launch)
   unsigned int* progress;  // per tile: completed time blocks (zeroed before the launch)
+  uint64_t wait_ns;        // bound of every progress wait
 };
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
@@ -67,15 +68,26 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Bounded wait until *p >= target.  Returns false on timeout (~2 s).
-__device__ __forceinline__ bool wait_at_least(const unsigned* p, unsigned target) {
+// Bounded wait until *p >= target.  Returns false after limit_ns, or at once
+// when the library's device error word is set (another wait gave up: the
+// launch's results are void, so no block spends its own limit on it).
+__device__ __forceinline__ bool wait_at_least(const unsigned* p, unsigned target, uint64_t limit_ns) {
   if (ld_acquire_gpu(p) >= target) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t it = 0;; ++it) {
     __nanosleep(100);
     if (ld_acquire_gpu(p) >= target) return true;
-    if ((it & 63u) == 63u && globaltimer_ns() - t0 > 2000000000ull) return false;
+    if ((it & 15u) == 15u &&
+        (globaltimer_ns() - t0 > limit_ns || *reinterpret_cast<const volatile int*>(&g_err) != 0))
+      return false;
   }
+}
+
+// Test hook of the bounded wait (pde_wait_probe): thread 0 waits until
+// *word >= target under the library's limit and records PDE_ERR_TIMEOUT if it
+// gives up.
+__global__ void wait_probe_kernel(const unsigned* word, unsigned target, uint64_t limit_ns) {
+  if (threadIdx.x == 0 && !wait_at_least(word, target, limit_ns)) flag_error(PDE_ERR_TIMEOUT);
 }
 
 template <int OP, int R>
@@ -107,7 +119,7 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
     if (tb > 0 && threadIdx.x < 9) {
       const int nx = tx + (int)threadIdx.x / 3 - 1, ny = ty + (int)threadIdx.x % 3 - 1;
       if (nx >= 0 && nx < tiles_x && ny >= 0 && ny < tiles_y && !timed_out) {
-        if (!wait_at_least(P.progress + Gd.tile_base + nx * tiles_y + ny, (unsigned)tb)) {
+        if (!wait_at_least(P.progress + Gd.tile_base + nx * tiles_y + ny, (unsigned)tb, P.wait_ns)) {
           timed_out = true;
           flag_error(PDE_ERR_TIMEOUT);
         }

@@ -27,6 +27,8 @@ int launch_status() { return cudaGetLastError() == cudaSuccess ? PDE_OK : PDE_ER
 // Launch shape of the temporally blocked 2D kernels set by pde_set_launch_2d
 // (tile sides, threads per block); 0 = each entry point's own choice.
 int g_tile2d[2] = {0, 0};
+// Bound of every device-side wait (pde_set_wait_limit_ns).
+uint64_t g_wait_ns = PDE_WAIT_LIMIT_DEFAULT_NS;
 int g_threads2d = 0;
 
 // A 2D tile count just above m x SMs (m = 1, 2) leaves a short tail wave in which
@@ -83,6 +85,7 @@ int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& 
   for (int t = 0; t < 5; ++t) P.w[t] = Wt.w[t];
   P.alpha = alpha;
   P.out = out;
+  P.wait_ns = g_wait_ns;
   // Persistent grid over (chunk, tile) items in chunk-major order.  The chunk
   // count is chosen by a load model: the busiest SM runs ceil(blocks/SMs)
   // blocks of ceil(items/blocks) items each, against the ideal items/SMs, and
@@ -273,6 +276,18 @@ const char* pde_strerror(int s) {
     case PDE_ERR_TOO_LARGE: return "size above the documented maximum";
     default: return "unknown status";
   }
+}
+
+uint64_t pde_set_wait_limit_ns(uint64_t ns) {
+  const uint64_t prev = g_wait_ns;
+  g_wait_ns = ns > 0 ? ns : PDE_WAIT_LIMIT_DEFAULT_NS;
+  return prev;
+}
+
+int pde_wait_probe(const uint32_t* word, uint32_t target, void* stream) {
+  if (!word) return PDE_ERR_ARG;
+  wait_probe_kernel<<<1, 32, 0, as_stream(stream)>>>(word, target, g_wait_ns);
+  return launch_status();
 }
 
 int pde_device_error(void* stream) {
@@ -1492,6 +1507,7 @@ int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream) {
   P.g = plan->ghost_cells;
   P.counter = reinterpret_cast<unsigned*>(base + table_bytes);
   P.progress = reinterpret_cast<unsigned*>(base + table_bytes + BATCH_QUEUE_OFF_ALIGN);
+  P.wait_ns = g_wait_ns;
   cudaStream_t st = as_stream(stream);
   PDE_CUDA_CHECK(cudaMemsetAsync(P.counter, 0, BATCH_QUEUE_OFF_ALIGN + (size_t)plan->total_tiles * sizeof(unsigned), st));
   const int64_t items = (int64_t)ntb * plan->total_tiles;

@@ -35,6 +35,7 @@ struct S3Params {
   float w[5];
   float alpha;
   float* out;
+  uint64_t wait_ns;     // bound of every mbarrier wait
 };
 
 __host__ __device__ constexpr int round4(int v) { return (v + 3) & ~3; }
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
       const int plane_f = P.Y * P.Z * CIN, row_f = P.Z * CIN;
       for (int i = 0; i < nplanes; ++i) {
         // plane `issued` reuses the stage of plane issued - S: wait for its release
-        if (issued >= S && !dead && !mbar_wait_bounded(&empty[s], (uint32_t)(ph ^ 1))) {
+        if (issued >= S && !dead && !mbar_wait_bounded(&empty[s], (uint32_t)(ph ^ 1), P.wait_ns, &g_err)) {
           dead = true;
           flag_error(PDE_ERR_TIMEOUT);
         }
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
   int ns = 0, nph = 0, cs = 0;
   auto adv = [&](int& st) { if (++st == S) st = 0; };
   auto wait_new = [&]() {
-    if (!dead && !mbar_wait_bounded(&full[ns], (uint32_t)nph)) {
+    if (!dead && !mbar_wait_bounded(&full[ns], (uint32_t)nph, P.wait_ns, &g_err)) {
       dead = true;
       flag_error(PDE_ERR_TIMEOUT);
     }

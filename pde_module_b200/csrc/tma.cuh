@@ -49,14 +49,18 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
   return t;
 }
 
-// Bounded wait on an mbarrier phase: gives up after ~2 s (or 2^26 polls) and
+// Bounded wait on an mbarrier phase: gives up after limit_ns (or 2^26 polls),
+// or at once when *err (the library's device error word) is already set, and
 // returns false; the caller records PDE_ERR_TIMEOUT and stops waiting.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint64_t limit_ns,
+                                                  const int* err) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = globaltimer_ns();
   for (uint32_t it = 0; it < (1u << 26); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
-    if ((it & 255u) == 255u && globaltimer_ns() - t0 > 2000000000ull) break;
+    if ((it & 255u) == 255u &&
+        (globaltimer_ns() - t0 > limit_ns || *reinterpret_cast<const volatile int*>(err) != 0))
+      break;
   }
   return false;
 }

@@ -16,7 +16,7 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 
 def header_symbols():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pde_\w+)\s*\(", txt, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|uint64_t|const char\*)\s+(pde_\w+)\s*\(", txt, flags=re.M)))
 
 
 def test_library_loads_and_exports_header_symbols():
