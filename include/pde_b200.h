@@ -528,8 +528,10 @@ int pde_layer_apply(const float* in, float* out, int32_t ncomp, const int64_t* c
  * scratch field comes from a fixed device array inside this library, of
  * PDE_NOALLOC_MAX_FLOATS floats (16 MiB), held on every GPU that loads the
  * library until the process exits.  Grids with X*Y*Z*ncomp above that return
- * PDE_ERR_TOO_LARGE.  The first call on a device looks the array up
- * (cudaGetSymbolAddress) and should come before any stream capture.  All calls
+ * PDE_ERR_TOO_LARGE.  The first call in a CUDA context looks the array up
+ * (cudaGetSymbolAddress) and should come before any stream capture; the
+ * address is kept per context (by its unique id), so a new context, or the
+ * primary context again after cudaDeviceReset, looks it up anew.  All calls
  * share the array: calls that overlap on the GPU race, so serialise them.
  * Arguments and results are those of pde_heat_rollout without `work`. */
 #define PDE_NOALLOC_MAX_FLOATS (1 << 22)
