@@ -267,6 +267,15 @@ int pde_heat_rollout_at(const float* u_in, float* u_out, float* work, const PdeG
 int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
                      const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
                      void* stream);
+/* pde_heat_forward with time-dependent groups (ramps, boundary_functions.py:77-92):
+ * step n of this call is rollout step n0 + n and fills the boundary at
+ * t = fp32(t0 + (n0 + n) * t_step), the sum and product in double, each rounded
+ * on its own, as a loop calling BC(u, t0 + k*dt) computes it.  pde_heat_forward
+ * refuses ramp groups (PDE_ERR_UNSUPPORTED).  The adjoint takes the same rules:
+ * the fill is affine in u, its values enter the forward only. */
+int pde_heat_forward_at(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                        const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass,
+                        float* lstates, double t0, double t_step, int32_t n0, void* stream);
 /* Discrete adjoint of nsteps forward steps: lam_in = dJ/du^N, lam_out =
  * dJ/du^0; grad_alpha += dJ/dalpha (accumulated in step order n = N-1..0);
  * lstates as written by pde_heat_forward for the same steps. */
@@ -297,6 +306,16 @@ typedef struct PdeLDCParams {
 int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid,
                     const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
                     const PdeLDCParams* params, int32_t nsteps, void* stream);
+/* pde_ldc_rollout with time-dependent groups (a ramped lid, as the reference's
+ * function-BC cavity, Benchmark/Functional_BC/LDC_Graph Function.py:44-113,
+ * with boundary_functions.py:77-92): step n (0-based) fills every velocity and
+ * pressure boundary of the step at t = fp32(t0 + n * t_step), the sum and
+ * product in double, each rounded on its own, as a loop calling the boundaries
+ * with that time computes it.  pde_ldc_rollout refuses ramp groups
+ * (PDE_ERR_UNSUPPORTED). */
+int pde_ldc_rollout_at(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid,
+                       const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
+                       const PdeLDCParams* params, int32_t nsteps, double t0, double t_step, void* stream);
 
 /* ---- weakly compressible flow, RK2 (new: the reference composes the step from
  * its modules, examples/LDC/LDC_RK2.py) ----
@@ -461,6 +480,13 @@ int pde_batch_plan(int32_t kind, const PdeBatchGrid* grids, int32_t ngrids, int3
 /* Advance every grid of the plan nsteps: one memset of the queue state and one
  * kernel launch, so it can be captured in a CUDA graph. */
 int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream);
+/* pde_batch_rollout for heat plans whose groups include ramps
+ * (boundary_functions.py:77-92): step n (0-based) of grid i fills its boundary
+ * at t = fp32(t0 + n * dt_i), dt_i the grid's float time step widened to double,
+ * as a per-grid loop calling the boundary with that time; each grid's result is
+ * bit-identical to pde_heat_rollout_at with those times.  pde_batch_rollout
+ * refuses such plans (PDE_ERR_UNSUPPORTED). */
+int pde_batch_rollout_at(const PdeBatchPlan* plan, int32_t nsteps, double t0, void* stream);
 
 /* ---- immersed boundary (FDM/boundary/immersedBoundary.py) ----
  * Solid regions inside the grid given by an int8 bitmask (X, Y, Z), nonzero =

@@ -267,16 +267,17 @@ def heat_rollout(u: np.ndarray, groups: list, dx: float, ghost: int, alpha: floa
     return u
 
 
-def heat_forward_field(alpha, u0, groups, dx, ghost, dt, nsteps, order=2, dtype=np.float32):
+def heat_forward_field(alpha, u0, groups, dx, ghost, dt, nsteps, order=2, dtype=np.float32, t0=0.0):
     """New (the reference's loop, examples/2D_Heat_Equation.py:57-65, has a scalar
     alpha): the heat step with a per-cell diffusivity field, one component,
         v = B(u);  S = L(v) (alpha 1);  u' = v + dt*(alpha o S).
-    alpha, u0: (X, Y, Z, 1).  Returns (u^N, [S^0, ..., S^{N-1}]), S as (X, Y, Z) arrays."""
+    alpha, u0: (X, Y, Z, 1).  Step n fills the boundary at t0 + n*dt (ramp groups).
+    Returns (u^N, [S^0, ..., S^{N-1}]), S as (X, Y, Z) arrays."""
     u = np.asarray(u0, dtype=dtype)
     a = np.asarray(alpha, dtype=dtype)
     S = []
-    for _ in range(nsteps):
-        v = bc_apply(u, groups, dx, ghost, dtype=dtype)
+    for n in range(nsteps):
+        v = bc_apply(u, groups, dx, ghost, t0 + n * dt, dtype=dtype)
         acc = laplacian(v, dx, ghost, 1.0, order, dtype)
         S.append(acc[..., 0].copy())
         u = forward_euler(v, a * acc, dt, dtype)
@@ -377,7 +378,7 @@ def stencil_at(u: np.ndarray, cells: np.ndarray, w: np.ndarray, axes_comps, alph
 
 
 # ------------------------------------------------- fractional-step cavity ---
-def ldc_step(u, p, u_groups, p_groups, dx, ghost, nu, dt, jacobi_iters, dtype=np.float32):
+def ldc_step(u, p, u_groups, p_groups, dx, ghost, nu, dt, jacobi_iters, dtype=np.float32, t=0.0):
     """One projection step composed of the reference operators (no reference
     counterpart: its cavity uses artificial compressibility,
     examples/LDC/LDC_Graph_Capture.py:71-90).  u (X,Y,1,2), p (X,Y,1,1).
@@ -386,13 +387,15 @@ def ldc_step(u, p, u_groups, p_groups, dx, ghost, nu, dt, jacobi_iters, dtype=np
         rhs = (1/dt)*Div(BC_u(u*))
         jacobi_iters x: p <- 0.25*(pW + pE + pS + pN - dx^2*rhs) on BC_p(p)
         u = BC_u(u*) + dt*Grad(BC_p(p), -1)
+
+    Every boundary of the step is filled at time t (ramp groups).
     """
-    u2 = bc_apply(u, u_groups, dx, ghost, dtype=dtype)
+    u2 = bc_apply(u, u_groups, dx, ghost, t, dtype=dtype)
     lap = laplacian(u2, dx, ghost, nu, dtype=dtype)
     G = grad(u2, dx, ghost, 1.0, dtype=dtype)  # (X,Y,1,2,2): row = component, column = axis
     conv = G[..., 0] * u2[..., 0:1] + G[..., 1] * u2[..., 1:2]
     us = forward_euler(u2, lap - conv, dt, dtype)
-    us_bc = bc_apply(us, u_groups, dx, ghost, dtype=dtype)
+    us_bc = bc_apply(us, u_groups, dx, ghost, t, dtype=dtype)
     dt32 = float(np.float32(dt))
     inv_dt = float(np.float32(1.0 / dt32)) if dtype == np.float32 else 1.0 / dt
     rhs = divergence(us_bc, dx, ghost, inv_dt, dtype=dtype)
@@ -400,13 +403,13 @@ def ldc_step(u, p, u_groups, p_groups, dx, ghost, nu, dt, jacobi_iters, dtype=np
     X, Y = u.shape[0], u.shape[1]
     c = (slice(ghost, X - ghost), slice(ghost, Y - ghost), 0, 0)
     for _ in range(jacobi_iters):
-        pb = bc_apply(p, p_groups, dx, ghost, dtype=dtype)
+        pb = bc_apply(p, p_groups, dx, ghost, t, dtype=dtype)
         new = pb.copy()
         s = ((pb[ghost - 1:X - ghost - 1, ghost:Y - ghost, 0, 0] + pb[ghost + 1:X - ghost + 1, ghost:Y - ghost, 0, 0])
              + pb[ghost:X - ghost, ghost - 1:Y - ghost - 1, 0, 0]) + pb[ghost:X - ghost, ghost + 1:Y - ghost + 1, 0, 0]
         new[c] = dtype(0.25) * (s - h2 * rhs[c])
         p = new
-    pb = bc_apply(p, p_groups, dx, ghost, dtype=dtype)
+    pb = bc_apply(p, p_groups, dx, ghost, t, dtype=dtype)
     gp = grad(pb, dx, ghost, -1.0, dtype=dtype)
     u_new = forward_euler(us_bc, gp, dt, dtype)
     return u_new, p

@@ -150,6 +150,9 @@ _SIGS = {
     "pde_ldc_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.POINTER(PdeBCRules),
                                   C.POINTER(PdeLDCParams), C.c_int32, C.c_void_p]),
+    "pde_ldc_rollout_at": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.POINTER(PdeBCRules),
+                                     C.POINTER(PdeLDCParams), C.c_int32, C.c_double, C.c_double, C.c_void_p]),
     "pde_ldc_slab_step": (C.c_int, [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.POINTER(PdeGrid), C.POINTER(PdeSlab), C.POINTER(PdeBCRules),
                                     C.POINTER(PdeBCRules), C.POINTER(PdeLDCParams), C.c_int32, C.c_int32,
@@ -169,6 +172,9 @@ _SIGS = {
     "pde_heat_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid),
                                    C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32, C.c_void_p,
                                    C.c_void_p]),
+    "pde_heat_forward_at": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid),
+                                      C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32, C.c_void_p,
+                                      C.c_double, C.c_double, C.c_int32, C.c_void_p]),
     "pde_heat_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.c_float, C.c_int32, C.c_int32,
                                    C.c_void_p, C.c_void_p]),
@@ -178,6 +184,7 @@ _SIGS = {
                                  C.POINTER(PdeBCRules), C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_uint64,
                                  C.POINTER(PdeBatchPlan), C.c_void_p]),
     "pde_batch_rollout": (C.c_int, [C.POINTER(PdeBatchPlan), C.c_int32, C.c_void_p]),
+    "pde_batch_rollout_at": (C.c_int, [C.POINTER(PdeBatchPlan), C.c_int32, C.c_double, C.c_void_p]),
     "pde_heat_rollout_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                            C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                            C.c_void_p]),

@@ -56,6 +56,8 @@ struct BatchParams {
   unsigned int* counter;   // work queue head (zeroed before the launch)
   unsigned int* progress;  // per tile: completed time blocks (zeroed before the launch)
   uint64_t wait_ns;        // bound of every progress wait
+  int ramp;                // heat: some groups are time-dependent (ramps)
+  double t0;               // heat ramps: step n of a grid fills its boundary at fp32(t0 + n * (double)dt)
 };
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
@@ -94,6 +96,8 @@ template <int OP, int R>
 __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];
   __shared__ int s_item;
+  __shared__ PdeBCRules SR;  // ramps: the rules with the current step's group values
+  if (OP == BATCH_HEAT && P.ramp && threadIdx.x == 0) SR = Rl;
   const unsigned total_items = (unsigned)P.total_tiles * (unsigned)P.ntb;
   const int q = P.nsteps / P.ntb, rmd = P.nsteps % P.ntb;
   const int H = P.H, g = P.g;
@@ -167,8 +171,17 @@ __global__ void __launch_bounds__(256) batched_kernel(const BatchParams P, const
       const int tlx0 = bx0 - rx0, tly0 = by0 - ry0;  // the tile in region coordinates
       BcPlan<2> bp;
       bc_plan(bp, HP, rx0, RX, ry0, RY);
+      const int n_first = tb * q + min(tb, rmd);  // rollout step of the block's first step
       for (int s = 0; s < ks; ++s) {
-        bc_fill_planned<1, 1>(A, bp, HP, Rl, rx0, RX, ry0, RY, dx32);
+        if (P.ramp) {  // this step's ramp values (the previous step's fill is behind the barrier)
+          const int gi = (int)threadIdx.x;
+          if (gi < Rl.ngroups && Rl.group[gi].func == PDE_BC_FUNC_RAMP) {
+            const float t = step_time(P.t0, (double)dt, n_first + s);
+            SR.group[gi].value = bc_value(PDE_BC_FUNC_RAMP, Rl.group[gi].value, Rl.group[gi].t_max, &t);
+          }
+          __syncthreads();
+        }
+        bc_fill_planned<1, 1>(A, bp, HP, P.ramp ? SR : Rl, rx0, RX, ry0, RY, dx32);
         // Step s only has to update the stencil cells within R (ks - 1 - s) + 1 of
         // the tile (the boundary fills read inward): the stencil rectangle cut to
         // that box; the cells outside it keep stale values nobody reads.

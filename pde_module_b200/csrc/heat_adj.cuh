@@ -44,6 +44,9 @@ struct HAParams {
   const float* lsts;   // adjoint: S^n at lsts + n*cells
   int ntop;            // adjoint: this pass runs n = ntop, ntop-1, ..., ntop-k+1
   float* galpha;       // adjoint: dJ/dalpha, accumulated in place
+  int ramp;            // forward: time-dependent groups
+  int n0;              // forward: rollout step of the pass's first step
+  double t0, tstep;    // forward ramps: step n fills the boundary at fp32(t0 + n * tstep)
 };
 
 __device__ __forceinline__ bool heat_stencil_cell(int x, int y, int X, int Y, int g) {
@@ -54,7 +57,7 @@ __device__ __forceinline__ bool heat_stencil_cell(int x, int y, int X, int Y, in
 template <int R, bool STORE>
 __device__ __forceinline__ float* heat_field_steps(const HAParams& P, const PdeBCRules& Rl, float* A, float* B,
                                                    const float* AL, int rx0, int RX, int ry0, int RY, int bx0,
-                                                   int by0, int OX, int OY) {
+                                                   int by0, int OX, int OY, PdeBCRules* SR) {
   H2Params HP;
   HP.X = P.X; HP.Y = P.Y; HP.g = P.g; HP.N = 1;
   const int g = P.g, X = P.X, Y = P.Y;
@@ -67,7 +70,15 @@ __device__ __forceinline__ float* heat_field_steps(const HAParams& P, const PdeB
   BcPlan<2> bp;  // the region is the same for every step of the pass
   bc_plan(bp, HP, rx0, RX, ry0, RY);
   for (int s = 0; s < P.k; ++s) {
-    bc_fill_planned<1, 1>(A, bp, HP, Rl, rx0, RX, ry0, RY, Rl.dx32);
+    if (SR) {  // ramps: this step's group values (the previous step's fill is behind the barrier)
+      const int gi = (int)threadIdx.x;
+      if (gi < Rl.ngroups && Rl.group[gi].func == PDE_BC_FUNC_RAMP) {
+        const float t = step_time(P.t0, P.tstep, P.n0 + s);
+        SR->group[gi].value = bc_value(PDE_BC_FUNC_RAMP, Rl.group[gi].value, Rl.group[gi].t_max, &t);
+      }
+      __syncthreads();
+    }
+    bc_fill_planned<1, 1>(A, bp, HP, SR ? *SR : Rl, rx0, RX, ry0, RY, Rl.dx32);
     float* Ls = STORE ? P.lst + (size_t)s * P.cells : nullptr;
     int lx = (int)threadIdx.x / SW, ly = (int)threadIdx.x - lx * SW;
     for (int c = threadIdx.x; c < SC; c += nt) {
@@ -99,6 +110,8 @@ template <int R>
 __global__ void __launch_bounds__(1024) heat2d_field_fwd_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                                 const HAParams P, const PdeBCRules Rl) {
   extern __shared__ __align__(16) float sm[];
+  __shared__ PdeBCRules SR;  // ramps: the rules with the current step's group values
+  if (P.ramp && threadIdx.x == 0) SR = Rl;
   const int tx = blockIdx.x / P.tiles_y, ty = blockIdx.x % P.tiles_y;
   const int bx0 = tx * P.TBX, by0 = ty * P.TBY;
   const int H = P.k * R + 1;
@@ -123,8 +136,9 @@ __global__ void __launch_bounds__(1024) heat2d_field_fwd_kernel(const float* __r
   }
   cp_async_wait_all();
   __syncthreads();
-  float* A = P.lst ? heat_field_steps<R, true>(P, Rl, A0, B0, AL, rx0, RX, ry0, RY, bx0, by0, OX, OY)
-                   : heat_field_steps<R, false>(P, Rl, A0, B0, AL, rx0, RX, ry0, RY, bx0, by0, OX, OY);
+  PdeBCRules* srp = P.ramp ? &SR : nullptr;
+  float* A = P.lst ? heat_field_steps<R, true>(P, Rl, A0, B0, AL, rx0, RX, ry0, RY, bx0, by0, OX, OY, srp)
+                   : heat_field_steps<R, false>(P, Rl, A0, B0, AL, rx0, RX, ry0, RY, bx0, by0, OX, OY, srp);
   const float* Bf = (A == A0) ? B0 : A0;  // the last boundary-filled level
   // output: stencil cells from the newest level, the others as last filled
   RectWalk wo(OY, (int)blockDim.x);

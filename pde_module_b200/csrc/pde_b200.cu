@@ -715,7 +715,6 @@ int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_
   if (G->ndims != 2 || G->n[2] != 1) return PDE_ERR_UNSUPPORTED;
   if (G->g < G->order / 2 || G->g < 1) return PDE_ERR_GHOST;
   if (rules->ncomp != 1) return PDE_ERR_ARG;
-  if (rules->has_ramp) return PDE_ERR_UNSUPPORTED;
   if (G->n[0] < 2 * G->g + 3 || G->n[1] < 2 * G->g + 3) return PDE_ERR_SHAPE;
   const Weights W = lap_weights(G->order, grid->dx);
   memset(P, 0, sizeof(*P));
@@ -735,6 +734,12 @@ int heat_diff_setup(const PdeGrid* grid, const PdeBCRules* rules, int steps_per_
 
 }  // namespace
 
+namespace {
+int heat_forward_run(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                     const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
+                     double t0, double tstep, int n0, void* stream);
+}  // namespace
+
 extern "C" {
 
 int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads) {
@@ -750,6 +755,26 @@ int pde_set_launch_2d(int32_t tile_x, int32_t tile_y, int32_t threads) {
 int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
                      const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
                      void* stream) {
+  if (rules && rules->has_ramp) return PDE_ERR_UNSUPPORTED;
+  return heat_forward_run(alpha, u_in, u_out, work, grid, rules, dt, nsteps, steps_per_pass, lstates, 0.0, 0.0, 0,
+                          stream);
+}
+
+int pde_heat_forward_at(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                        const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
+                        double t0, double t_step, int32_t n0, void* stream) {
+  if (n0 < 0) return PDE_ERR_ARG;
+  return heat_forward_run(alpha, u_in, u_out, work, grid, rules, dt, nsteps, steps_per_pass, lstates, t0, t_step, n0,
+                          stream);
+}
+
+}  // extern "C"
+
+namespace {
+
+int heat_forward_run(const float* alpha, const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                     const PdeBCRules* rules, float dt, int32_t nsteps, int32_t steps_per_pass, float* lstates,
+                     double t0, double tstep, int n0, void* stream) {
   if (!alpha || !u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
   if (work == u_in || work == u_out) return PDE_ERR_ARG;
   Geo G;
@@ -774,6 +799,9 @@ int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float*
   const int threads = pick_threads_2d(tiles);
   P.alpha = alpha;
   P.dt = dt;
+  P.ramp = rules->has_ramp ? 1 : 0;
+  P.t0 = t0;
+  P.tstep = tstep;
   const int npasses = (nsteps + k - 1) / k;
   const bool alias = (u_out == u_in);
   const float* src = u_in;
@@ -782,6 +810,7 @@ int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float*
   for (int p = 0; p < npasses; ++p) {
     P.k = (nsteps - done < k) ? (nsteps - done) : k;
     P.lst = lstates ? lstates + (size_t)done * P.cells : nullptr;
+    P.n0 = n0 + done;
     kern<<<tiles, threads, smem, st>>>(src, dst, P, *rules);
     rc = launch_status();
     if (rc) return rc;
@@ -792,6 +821,10 @@ int pde_heat_forward(const float* alpha, const float* u_in, float* u_out, float*
   if (src != u_out) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, src, bytes, cudaMemcpyDeviceToDevice, st));
   return PDE_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 int pde_heat_adjoint(const float* alpha, const float* lam_in, float* lam_out, const float* lstates,
                      float* grad_alpha, const PdeGrid* grid, const PdeBCRules* rules, float dt, int32_t nsteps,
@@ -1075,9 +1108,10 @@ namespace {
 
 // Checks and constants shared by the cavity entry points; G describes the whole domain.
 int ldc_setup(const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules, const PdeLDCParams* prm,
-              Geo* G, LdcConst* K) {
+              Geo* G, LdcConst* K, bool allow_ramp = false) {
   if (!grid || !u_rules || !p_rules || !prm) return PDE_ERR_ARG;
-  if (u_rules->ncomp != 2 || p_rules->ncomp != 1 || u_rules->has_ramp || p_rules->has_ramp) return PDE_ERR_ARG;
+  if (u_rules->ncomp != 2 || p_rules->ncomp != 1) return PDE_ERR_ARG;
+  if (!allow_ramp && (u_rules->has_ramp || p_rules->has_ramp)) return PDE_ERR_UNSUPPORTED;
   if (prm->jacobi_iters < 0 || prm->jacobi_per_pass < 0) return PDE_ERR_ARG;
   if (!make_geo(grid, G)) return PDE_ERR_SHAPE;
   if (G->ndims != 2 || G->n[2] != 1 || grid->order != 2) return PDE_ERR_UNSUPPORTED;
@@ -1162,15 +1196,24 @@ int launch_jacobi(const JacobiLaunch& L, cudaStream_t st, const float* pin, floa
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid, const PdeGrid* grid,
-                    const PdeBCRules* u_rules, const PdeBCRules* p_rules, const PdeLDCParams* prm, int32_t nsteps,
-                    void* stream) {
+// The rules of step n: ramp groups take their value at fp32(t0 + n * tstep).
+PdeBCRules rules_at(const PdeBCRules& R, double t0, double tstep, long long n) {
+  PdeBCRules out = R;
+  if (R.has_ramp)
+    for (int i = 0; i < R.ngroups; ++i)
+      if (R.group[i].func == PDE_BC_FUNC_RAMP) out.group[i].value = host_ramp_value(R.group[i], t0, tstep, n);
+  return out;
+}
+
+int ldc_rollout_run(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid, const PdeGrid* grid,
+                    const PdeBCRules* u_rules_in, const PdeBCRules* p_rules_in, const PdeLDCParams* prm,
+                    int32_t nsteps, bool allow_ramp, double t0, double tstep, void* stream) {
   if (!u || !p || !u_star || !p_tmp || !rhs || nsteps < 0) return PDE_ERR_ARG;
   Geo G;
   LdcConst K;
-  int rc = ldc_setup(grid, u_rules, p_rules, prm, &G, &K);
+  int rc = ldc_setup(grid, u_rules_in, p_rules_in, prm, &G, &K, allow_ramp);
   if (rc) return rc;
   cudaStream_t st = as_stream(stream);
   const int64_t cells = G.n[0] * G.n[1];
@@ -1185,6 +1228,10 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
   rc = jacobi_setup(G, K.h2, k, 0, X, 0, X, &JP, &JL);
   if (rc) return rc;
   for (int step = 0; step < nsteps; ++step) {
+    // time-dependent groups: step n fills every boundary at t0 + n * tstep
+    const PdeBCRules ur = rules_at(*u_rules_in, t0, tstep, step), pr = rules_at(*p_rules_in, t0, tstep, step);
+    const PdeBCRules* u_rules = &ur;
+    const PdeBCRules* p_rules = &pr;
     ldc_predictor_kernel<<<grid2, 256, 0, st>>>(u, u_star, G, *u_rules, K, 0);
     ldc_divergence_kernel<<<grid2, 256, 0, st>>>(u_star, rhs, G, *u_rules, K, 0);
     float* src = p;
@@ -1206,6 +1253,25 @@ int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs,
   }
   return PDE_OK;
 }
+
+}  // namespace
+
+extern "C" {
+
+int pde_ldc_rollout(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid, const PdeGrid* grid,
+                    const PdeBCRules* u_rules, const PdeBCRules* p_rules, const PdeLDCParams* prm, int32_t nsteps,
+                    void* stream) {
+  return ldc_rollout_run(u, p, u_star, p_tmp, rhs, resid, grid, u_rules, p_rules, prm, nsteps, false, 0.0, 0.0,
+                         stream);
+}
+
+int pde_ldc_rollout_at(float* u, float* p, float* u_star, float* p_tmp, float* rhs, float* resid,
+                       const PdeGrid* grid, const PdeBCRules* u_rules, const PdeBCRules* p_rules,
+                       const PdeLDCParams* prm, int32_t nsteps, double t0, double t_step, void* stream) {
+  return ldc_rollout_run(u, p, u_star, p_tmp, rhs, resid, grid, u_rules, p_rules, prm, nsteps, true, t0, t_step,
+                         stream);
+}
+
 
 int pde_wc_rk2(const float* m_in, const float* rho_in, float* m_out, float* rho_out, const PdeGrid* grid,
                const PdeBCRules* u_rules, const PdeBCRules* rho_rules, const PdeWCParams* prm, int32_t nsteps,
@@ -1388,6 +1454,10 @@ int batch_occupancy(int smem, int* occ) {
 
 }  // namespace
 
+namespace {
+int batch_rollout_run(const PdeBatchPlan* plan, int32_t nsteps, double t0, void* stream);
+}  // namespace
+
 extern "C" {
 
 int pde_batch_work_bytes(const PdeBatchGrid* grids, int32_t ngrids, int32_t tile_x, int32_t tile_y,
@@ -1412,7 +1482,6 @@ int pde_batch_plan(int32_t kind, const PdeBatchGrid* grids, int32_t ngrids, int3
   if (kind == PDE_BATCH_HEAT) {
     if (!rules) return PDE_ERR_ARG;
     if (rules->ncomp != 1) return PDE_ERR_ARG;
-    if (rules->has_ramp) return PDE_ERR_UNSUPPORTED;
   }
   if ((reinterpret_cast<uintptr_t>(work) & (BATCH_QUEUE_OFF_ALIGN - 1)) != 0) return PDE_ERR_ALIGN;
   const int tx = tile_x > 0 ? tile_x : BATCH_TILE_X, ty = tile_y > 0 ? tile_y : BATCH_TILE_Y;
@@ -1484,6 +1553,19 @@ int pde_batch_plan(int32_t kind, const PdeBatchGrid* grids, int32_t ngrids, int3
 }
 
 int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream) {
+  if (plan && plan->kind == PDE_BATCH_HEAT && plan->rules.has_ramp) return PDE_ERR_UNSUPPORTED;
+  return batch_rollout_run(plan, nsteps, 0.0, stream);
+}
+
+int pde_batch_rollout_at(const PdeBatchPlan* plan, int32_t nsteps, double t0, void* stream) {
+  return batch_rollout_run(plan, nsteps, t0, stream);
+}
+
+}  // extern "C"
+
+namespace {
+
+int batch_rollout_run(const PdeBatchPlan* plan, int32_t nsteps, double t0, void* stream) {
   if (!plan || !plan->table || nsteps < 0 || plan->steps_per_pass < 1 || plan->total_tiles < 1) return PDE_ERR_ARG;
   if (nsteps == 0) return PDE_OK;
   const int k = plan->steps_per_pass;
@@ -1508,6 +1590,8 @@ int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream) {
   P.counter = reinterpret_cast<unsigned*>(base + table_bytes);
   P.progress = reinterpret_cast<unsigned*>(base + table_bytes + BATCH_QUEUE_OFF_ALIGN);
   P.wait_ns = g_wait_ns;
+  P.ramp = (plan->kind == PDE_BATCH_HEAT && plan->rules.has_ramp) ? 1 : 0;
+  P.t0 = t0;
   cudaStream_t st = as_stream(stream);
   PDE_CUDA_CHECK(cudaMemsetAsync(P.counter, 0, BATCH_QUEUE_OFF_ALIGN + (size_t)plan->total_tiles * sizeof(unsigned), st));
   const int64_t items = (int64_t)ntb * plan->total_tiles;
@@ -1522,4 +1606,4 @@ int pde_batch_rollout(const PdeBatchPlan* plan, int32_t nsteps, void* stream) {
   return launch_status();
 }
 
-}  // extern "C"
+}  // namespace

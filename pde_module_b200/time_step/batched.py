@@ -118,9 +118,14 @@ class _BatchedRollout:
         """Array cells (ghosts included) of all grids."""
         return sum(int(f.shape[0]) * int(f.shape[1]) for f in self.fields)
 
-    def __call__(self, nsteps: int) -> list[torch.Tensor]:
-        check(lib().pde_batch_rollout(C.byref(self._plan), int(nsteps), C.c_void_p(stream_ptr(self.fields[0]))),
-              "pde_batch_rollout")
+    def __call__(self, nsteps: int, t0: float = 0.0) -> list[torch.Tensor]:
+        """Advance every grid nsteps.  Heat with time-ramped groups: step n of grid i
+        fills its boundary at t0 + n*dt_i (dt_i as a float32)."""
+        s = C.c_void_p(stream_ptr(self.fields[0]))
+        if self._rules is not None and self._rules.has_ramp:
+            check(lib().pde_batch_rollout_at(C.byref(self._plan), int(nsteps), float(t0), s), "pde_batch_rollout_at")
+        else:
+            check(lib().pde_batch_rollout(C.byref(self._plan), int(nsteps), s), "pde_batch_rollout")
         return self.fields
 
     def graph(self, nsteps: int) -> torch.cuda.CUDAGraph:
@@ -153,8 +158,6 @@ class BatchedHeatRollout(_BatchedRollout):
             boundary.dirichlet_BC("ALL", 0.0)
         if boundary.inputs[0] != 1:
             raise ValueError("batched heat rollouts take scalar fields")
-        if boundary.time_dependent:
-            raise NotImplementedError("batched heat rollouts take constant-valued boundary groups")
         self.boundary = boundary
         self._setup(fields, None, dx, alpha, dt, boundary.rules(), ghost_cells, order, tile, steps_per_pass)
 

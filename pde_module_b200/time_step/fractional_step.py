@@ -28,7 +28,11 @@ from ..FDM.boundary import GridBoundary
 class FractionalStepLDC:
     def __init__(self, n: int = 1024, Re: float = 100.0, lid: float = 1.0, cfl: float = 0.2,
                  jacobi_iters: int = 50, jacobi_per_pass: int = 0, ghost_cells: int = 1, device="cuda",
-                 dt: float | None = None) -> None:
+                 dt: float | None = None, lid_ramp_time: float | None = None) -> None:
+        """lid_ramp_time: the lid speed ramps from 0 to ``lid`` over this time
+        (boundary_functions.py:77-92), as the reference's function-BC cavity
+        does (Benchmark/Functional_BC/LDC_Graph Function.py:44-113); step n fills
+        its boundaries at t = n*dt from the first step of this solver."""
         g = int(ghost_cells)
         self.n, self.g = int(n), g
         self.dx = 1.0 / (n - 1)            # node-centred, n nodes from 0 to 1
@@ -41,10 +45,15 @@ class FractionalStepLDC:
         self.p = torch.zeros(shape + (1,), dtype=torch.float32, device=device)
         self.u_bc = GridBoundary(self.u, self.dx, g)
         self.u_bc.dirichlet_BC("ALL", 0.0)
-        self.u_bc.dirichlet_BC("+Y", self.lid, 0)
+        if lid_ramp_time:
+            from ..FDM.boundary import get_ramp_func
+            self.u_bc.dirichlet_BC("+Y", get_ramp_func(self.lid, float(lid_ramp_time), output_ids=(0,)), 0)
+        else:
+            self.u_bc.dirichlet_BC("+Y", self.lid, 0)
         self.p_bc = GridBoundary(self.p, self.dx, g)
         self.p_bc.vonNeumann_BC("ALL", 0.0)
         self.params = PdeLDCParams(self.nu, self.dt, int(jacobi_iters), int(jacobi_per_pass))
+        self.steps_done = 0
         self.grid = make_grid(shape, g, 2, self.dx)
         self._u_star = torch.zeros_like(self.u)
         self._p_tmp = torch.zeros_like(self.p)
@@ -67,11 +76,15 @@ class FractionalStepLDC:
             if self.residuals is None or self.residuals.numel() < nsteps:
                 self.residuals = torch.zeros(max(nsteps, 1), dtype=torch.float32, device=self.u.device)
             rp = C.c_void_p(self.residuals.data_ptr())
-        check(lib().pde_ldc_rollout(C.c_void_p(self.u.data_ptr()), C.c_void_p(self.p.data_ptr()),
-                                    C.c_void_p(self._u_star.data_ptr()), C.c_void_p(self._p_tmp.data_ptr()),
-                                    C.c_void_p(self._rhs.data_ptr()), rp, C.byref(self.grid),
-                                    C.byref(self.u_bc.rules()), C.byref(self.p_bc.rules()), C.byref(self.params),
-                                    int(nsteps), C.c_void_p(stream_ptr(self.u))), "pde_ldc_rollout")
+        args = [C.c_void_p(self.u.data_ptr()), C.c_void_p(self.p.data_ptr()), C.c_void_p(self._u_star.data_ptr()),
+                C.c_void_p(self._p_tmp.data_ptr()), C.c_void_p(self._rhs.data_ptr()), rp, C.byref(self.grid),
+                C.byref(self.u_bc.rules()), C.byref(self.p_bc.rules()), C.byref(self.params), int(nsteps)]
+        if self.u_bc.time_dependent:
+            check(lib().pde_ldc_rollout_at(*args, self.steps_done * self.dt, self.dt, C.c_void_p(stream_ptr(self.u))),
+                  "pde_ldc_rollout_at")
+        else:
+            check(lib().pde_ldc_rollout(*args, C.c_void_p(stream_ptr(self.u))), "pde_ldc_rollout")
+        self.steps_done += int(nsteps)
         return self.u, self.p
 
 

@@ -81,9 +81,8 @@ class HeatSolver:
         self.shape = tuple(boundary.grid_shape)
         assert self.shape[2] == 1 and self.shape[0] > 1 and self.shape[1] > 1, "2D grids (X, Y, 1)"
         self.dx, self.dt, self.N, self.order = float(dx), float(dt), int(nsteps), int(order)
-        if boundary.time_dependent:
-            raise NotImplementedError("HeatSolver takes constant-valued boundary groups")
         self.rules = boundary.rules()
+        self._t0 = 0.0  # ramp groups: step n fills the boundary at t0 + n*dt
         self.grid = make_grid(self.shape, boundary.ghost_cells, self.order, self.dx)
         self._steps_per_pass = int(steps_per_pass)
         self.graphs = bool(graphs)
@@ -139,14 +138,16 @@ class HeatSolver:
         self._seq_f.reset()
         self._seq_b.reset()
 
-    def _fwd(self, alpha, u, out, nsteps, lstates=None, work=None):
+    def _fwd(self, alpha, u, out, nsteps, lstates=None, work=None, n0=0):
         work = self._work if work is None else work
-        check(lib().pde_heat_forward(C.c_void_p(alpha.data_ptr()), C.c_void_p(u.data_ptr()),
-                                     C.c_void_p(out.data_ptr()), C.c_void_p(work.data_ptr()),
-                                     C.byref(self.grid), C.byref(self.rules), self.dt, int(nsteps),
-                                     self.steps_per_pass,
-                                     C.c_void_p(lstates.data_ptr()) if lstates is not None else None,
-                                     C.c_void_p(stream_ptr(u))), "pde_heat_forward")
+        args = [C.c_void_p(alpha.data_ptr()), C.c_void_p(u.data_ptr()), C.c_void_p(out.data_ptr()),
+                C.c_void_p(work.data_ptr()), C.byref(self.grid), C.byref(self.rules), self.dt, int(nsteps),
+                self.steps_per_pass, C.c_void_p(lstates.data_ptr()) if lstates is not None else None]
+        if self.rules.has_ramp:
+            check(lib().pde_heat_forward_at(*args, self._t0, self.dt, int(n0), C.c_void_p(stream_ptr(u))),
+                  "pde_heat_forward_at")
+        else:
+            check(lib().pde_heat_forward(*args, C.c_void_p(stream_ptr(u))), "pde_heat_forward")
 
     def _check(self, alpha, u):
         require_cuda_f32(alpha, "alpha")
@@ -158,7 +159,7 @@ class HeatSolver:
         for j, (n0, m) in enumerate(self.segments):
             last = j == len(self.segments) - 1
             self._fwd(self._alpha, self._ck[j], self._out if last else self._ck[j + 1], m,
-                      self._seg[:m] if last else None)
+                      self._seg[:m] if last else None, n0=n0)
         if not self.segments:
             self._out.copy_(self._ck[0])
 
@@ -181,7 +182,7 @@ class HeatSolver:
                     if j + 1 in adj_done:
                         side.wait_event(adj_done[j + 1])  # its buffer was segment j+1's
                     self._fwd(self._alpha, self._ck[j - 1], self._tmp, m, bufs[(J - j + 1) % 2][:m],
-                              work=self._work_r)
+                              work=self._work_r, n0=n0)
                     rec_done[j - 1] = torch.cuda.Event()
                     rec_done[j - 1].record(side)
             n0, m = self.segments[j]
@@ -198,10 +199,16 @@ class HeatSolver:
             a, b = b, a
         main.wait_stream(side)
 
-    def forward(self, alpha: torch.Tensor, u0: torch.Tensor) -> torch.Tensor:
-        """u^N for diffusivity field alpha and initial field u0."""
+    def forward(self, alpha: torch.Tensor, u0: torch.Tensor, t0: float = 0.0) -> torch.Tensor:
+        """u^N for diffusivity field alpha and initial field u0; with time-ramped
+        groups step n fills the boundary at t0 + n*dt (a new t0 re-captures the
+        sequences' graphs, which hold the times)."""
         self._check(alpha, u0)
         self._buffers(u0)
+        if self.rules.has_ramp and float(t0) != self._t0:
+            self._t0 = float(t0)
+            self._seq_f.reset()
+            self._seq_b.reset()
         self._alpha.copy_(alpha)
         self._ck[0].copy_(u0)
         self._seq_f.run()
@@ -222,19 +229,20 @@ class HeatSolver:
 
 class _HeatFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, alpha, u0, solver):
+    def forward(ctx, alpha, u0, solver, t0):
         ctx.solver = solver
         ctx.save_for_backward(alpha)
-        return solver.forward(alpha.detach().contiguous(), u0.detach().contiguous())
+        return solver.forward(alpha.detach().contiguous(), u0.detach().contiguous(), t0)
 
     @staticmethod
     def backward(ctx, g):
         (alpha,) = ctx.saved_tensors
         ga, gu = ctx.solver.backward(alpha.detach().contiguous(), g.contiguous())
-        return ga, gu, None
+        return ga, gu, None, None
 
 
-def heat_rollout(alpha: torch.Tensor, u0: torch.Tensor, solver: HeatSolver) -> torch.Tensor:
+def heat_rollout(alpha: torch.Tensor, u0: torch.Tensor, solver: HeatSolver, t0: float = 0.0) -> torch.Tensor:
     """u^N as a differentiable function of the diffusivity field alpha and u0
-    (a scalar alpha can be broadcast: ``alpha_s.expand(shape)`` sums its gradient)."""
-    return _HeatFn.apply(alpha, u0, solver)
+    (a scalar alpha can be broadcast: ``alpha_s.expand(shape)`` sums its gradient);
+    time-ramped groups are filled at t0 + n*dt."""
+    return _HeatFn.apply(alpha, u0, solver, float(t0))

@@ -211,9 +211,13 @@ def test_batch_plan_validation_needs_no_gpu():
     assert plan_rc(tx=256, ty=256, k=16) == _lib.PDE_ERR_TOO_LARGE  # shared-memory region too large
     tiny = _batch_desc([(3, 40)])
     assert plan_rc(d=tiny, n=1) == _lib.PDE_ERR_SHAPE
-    ramp = _lib.PdeBCRules.from_buffer_copy(rules)
-    ramp.has_ramp = 1
-    assert plan_rc(r=ramp) == _lib.PDE_ERR_UNSUPPORTED
+    # a heat plan with ramp groups runs only through pde_batch_rollout_at
+    ramp_plan = _lib.PdeBatchPlan()
+    ramp_plan.table = 1 << 24
+    ramp_plan.kind, ramp_plan.steps_per_pass, ramp_plan.total_tiles = _lib.PDE_BATCH_HEAT, 4, 1
+    ramp_plan.rules.has_ramp = 1
+    assert L.pde_batch_rollout(C.byref(ramp_plan), 5, None) == _lib.PDE_ERR_UNSUPPORTED
+    assert L.pde_batch_rollout_at(None, 5, 0.0, None) == _lib.PDE_ERR_ARG
     assert L.pde_batch_rollout(None, 5, None) == _lib.PDE_ERR_ARG
     assert L.pde_batch_rollout(C.byref(_lib.PdeBatchPlan()), 5, None) == _lib.PDE_ERR_ARG
 
