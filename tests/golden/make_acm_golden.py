@@ -30,8 +30,11 @@ OUT = os.path.join(HERE, "acm_golden.npz")
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PDE_MODULE_REFERENCE"),
+                    help="root of the PDE_Module source tree (or set PDE_MODULE_REFERENCE)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set PDE_MODULE_REFERENCE to the PDE_Module source tree")
 
     sys.path.insert(0, HERE)
     import warp_emu
