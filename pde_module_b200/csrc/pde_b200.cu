@@ -86,6 +86,7 @@ int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& 
   P.alpha = alpha;
   P.out = out;
   P.wait_ns = g_wait_ns;
+  P.negzero = -0.0f;
   // Persistent grid over (chunk, tile) items in chunk-major order.  The chunk
   // count is chosen by a load model: the busiest SM runs ceil(blocks/SMs)
   // blocks of ceil(items/blocks) items each, against the ideal items/SMs, and

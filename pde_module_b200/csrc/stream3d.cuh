@@ -36,6 +36,7 @@ struct S3Params {
   float alpha;
   float* out;
   uint64_t wait_ns;     // bound of every mbarrier wait
+  float negzero;        // -0.0f: the addend of the packed products (not a compile-time constant)
 };
 
 __host__ __device__ constexpr int round4(int v) { return (v + 3) & ~3; }
@@ -176,6 +177,10 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
 #pragma unroll
   for (int t = 0; t < T; ++t) w[t] = P.w[t];
   const float alpha = P.alpha;
+  float2 w2[T];
+#pragma unroll
+  for (int t = 0; t < T; ++t) w2[t] = make_float2(w[t], w[t]);
+  const float2 al2 = make_float2(alpha, alpha), nz2 = make_float2(P.negzero, P.negzero);
 
   bool dead = false;
   // consumer stage counters: the newest plane (ns, nph) and the centre plane (cs)
@@ -279,36 +284,56 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
           rf0 = (((size_t)(xs + j) * P.Y + y0) * P.Z + z0) * 3;
           r0 = (obase + (int)(rf0 & 31u)) & 31;
         }
+        if constexpr (MODE == MODE_EXACT) {
+          // Two rows per lane pair: packed products (__ffma2_rn with a run-time -0
+          // addend, the correctly rounded product) and sums (__fadd2_rn), each lane
+          // the scalar operation of the reference order.
+          static_assert(YPT % 2 == 0, "row pairs");
 #pragma unroll
-        for (int k = 0; k < YPT; ++k) {
-          const float* rowp = sc + rowoff(R + k) + off[(R + k) & 3] + zcmp;
-          auto xq = [&](int t) { return q[(jj + t) % T][k]; };
-          auto zt = [&](int t) { return (t == R && OP == OP_LAP) ? col[k + R] : rowp[(t - R) * zstep]; };
-          if constexpr (MODE == MODE_EXACT) {
+          for (int kp = 0; kp < YPT; kp += 2) {
+            const float* rp0 = sc + rowoff(R + kp) + off[(R + kp) & 3] + zcmp;
+            const float* rp1 = sc + rowoff(R + kp + 1) + off[(R + kp + 1) & 3] + zcmp;
+            auto X2 = [&](int t) { return make_float2(q[(jj + t) % T][kp], q[(jj + t) % T][kp + 1]); };
+            auto Y2 = [&](int t) { return make_float2(col[kp + t], col[kp + 1 + t]); };
+            auto Z2 = [&](int t) {
+              if (t == R && OP != OP_DIV) return make_float2(col[kp + R], col[kp + 1 + R]);
+              return make_float2(rp0[(t - R) * zstep], rp1[(t - R) * zstep]);
+            };
+            auto M2 = [&](float2 a, float2 b) { return __ffma2_rn(a, b, nz2); };
             if constexpr (OP == OP_LAP || OP == OP_DIV) {
-              float acc = mul(w[0], xq(0));
+              float2 acc = M2(w2[0], X2(0));
 #pragma unroll
-              for (int t = 1; t < T; ++t) acc = add(acc, mul(w[t], xq(t)));
+              for (int t = 1; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], X2(t)));
 #pragma unroll
-              for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], col[k + t]));
+              for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], Y2(t)));
 #pragma unroll
-              for (int t = 0; t < T; ++t) acc = add(acc, mul(w[t], zt(t)));
-              res[k][0] = mul(alpha, acc);
+              for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], Z2(t)));
+              const float2 r = M2(al2, acc);
+              res[kp][0] = r.x;
+              res[kp + 1][0] = r.y;
             } else {
-              float ax = mul(w[0], xq(0));
+              float2 ax = M2(w2[0], X2(0)), ay = M2(w2[0], Y2(0)), az = M2(w2[0], Z2(0));
 #pragma unroll
-              for (int t = 1; t < T; ++t) ax = add(ax, mul(w[t], xq(t)));
-              float ay = mul(w[0], col[k]);
-#pragma unroll
-              for (int t = 1; t < T; ++t) ay = add(ay, mul(w[t], col[k + t]));
-              float az = mul(w[0], rowp[-R * zstep]);
-#pragma unroll
-              for (int t = 1; t < T; ++t) az = add(az, mul(w[t], t == R ? col[k + R] : rowp[(t - R) * zstep]));
-              res[k][0] = mul(alpha, ax);
-              res[k][1] = mul(alpha, ay);
-              res[k][2] = mul(alpha, az);
+              for (int t = 1; t < T; ++t) {
+                ax = __fadd2_rn(ax, M2(w2[t], X2(t)));
+                ay = __fadd2_rn(ay, M2(w2[t], Y2(t)));
+                az = __fadd2_rn(az, M2(w2[t], Z2(t)));
+              }
+              const float2 rx = M2(al2, ax), ry = M2(al2, ay), rz = M2(al2, az);
+              res[kp][0] = rx.x;
+              res[kp + 1][0] = rx.y;
+              res[kp][1] = ry.x;
+              res[kp + 1][1] = ry.y;
+              res[kp][2] = rz.x;
+              res[kp + 1][2] = rz.y;
             }
-          } else {
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < YPT; ++k) {
+            const float* rowp = sc + rowoff(R + k) + off[(R + k) & 3] + zcmp;
+            auto xq = [&](int t) { return q[(jj + t) % T][k]; };
+            auto zt = [&](int t) { return (t == R && OP == OP_LAP) ? col[k + R] : rowp[(t - R) * zstep]; };
             if constexpr (OP == OP_LAP) {
               // alpha*(sum_t w[t]*(x,y,z taps)) = a[R]*centre + sum_{t<R} a[t]*(six mirrored taps)
               float acc = FW.a[R] * col[k + R];
@@ -345,7 +370,10 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>::TH
               res[k][2] = az;
             }
           }
-          if constexpr (OP == OP_GRAD) {  // staged at once: the row's results need no registers after this
+        }
+        if constexpr (OP == OP_GRAD) {  // staged: the rows' results need no registers after this
+#pragma unroll
+          for (int k = 0; k < YPT; ++k) {
             const int t = row0 + k;
             float* sr = ob + t * C::OROW + ((r0 + t * dzr) & 31) + 3 * lane;
             sr[0] = res[k][0];
