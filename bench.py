@@ -1139,6 +1139,8 @@ def run_profile_op(args):
     import pde_module_b200 as P
     if args.profile_op in ("wave", "heatadj", "batched", "ldc", "heat"):
         return run_profile_2d(args)
+    if args.profile_op in ("heat3d_o2", "heat3d_o4"):
+        return run_profile_heat3d(args)
     op, order = args.profile_op[:-1], int(args.profile_op[-1])
     n = args.profile_n
     g = order // 2
@@ -1166,6 +1168,35 @@ def run_profile_op(args):
     ms = e0.elapsed_time(e1) / args.iters
     b = {"lap": 8, "grad": 16, "div": 16}[op]
     print(json.dumps({"profile_op": args.profile_op, "n": n, "ms": ms, "gbs": n ** 3 * b / ms / 1e6}))
+    return 0
+
+
+def run_profile_heat3d(args):
+    """The fused 3D heat rollout for profilers: --profile-n^3 interior, order 2 or 4,
+    Dirichlet 0 on all faces, --profile-k steps per pass (0: 4 for order 2, 2 for
+    order 4), each of --iters calls one pass (k steps)."""
+    import torch
+    import pde_module_b200 as P
+    order = int(args.profile_op[-1])
+    n, g = args.profile_n, order // 2
+    k = args.profile_k or (4 if order == 2 else 2)
+    dx = 1.0 / (n - 1)
+    u = torch.rand((n + 2 * g,) * 3 + (1,), device="cuda")
+    bc = P.GridBoundary(u, dx, g)
+    bc.dirichlet_BC("ALL", 0.0)
+    roll = P.HeatRollout(bc, dx, 1.0, 0.15 * dx * dx, order=order, steps_per_pass=k)
+    for _ in range(2):
+        roll(u, k)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.iters):
+        roll(u, k)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (args.iters * k)
+    print(json.dumps({"profile_op": args.profile_op, "n": n, "k": k, "ms_per_step": ms,
+                      "cell_updates_per_s": n ** 3 / (ms / 1e3)}))
     return 0
 
 
@@ -1237,6 +1268,7 @@ def main():
     ap.add_argument("--profile-op", default=None, help="run one operator only (lap2, grad4, div2, ...)")
     ap.add_argument("--profile-n", type=int, default=N_INT)
     ap.add_argument("--profile-fast", action="store_true")
+    ap.add_argument("--profile-k", type=int, default=0, help="heat3d_o2/o4: steps per pass")
     ap.add_argument("--iters", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":

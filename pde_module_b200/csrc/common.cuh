@@ -15,6 +15,11 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
   const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(valid ? 4 : 0) : "memory");
 }
+// Asynchronous 8-byte global -> shared copy (both addresses 8-byte aligned).
+__device__ __forceinline__ void cp_async8(float* dst, const float* src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
 // Wait for this thread's cp.async copies (the block still needs a barrier before others read them).
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 

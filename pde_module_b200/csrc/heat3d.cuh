@@ -73,9 +73,12 @@ template <int R, int K, int N, int TYM, int TZM, int T>
 struct H3Cfg {
   static constexpr int H = K * R + 1;                     // region halo
   static constexpr int RYM = TYM + 2 * H;                 // region rows (max)
-  static constexpr int P = ((TZM + 2 * H) * N + 2 + 7) & ~7;  // row pitch (floats): row + even-start lead
+  static constexpr int PW = ((TZM + 2 * H) * N + 2 + 7) & ~7;  // row width (floats): row + even-start lead
+  // Row pitch: 8 mod 16 floats, so the four rows of a half warp's pair loads
+  // (lanes 4r..4r+3 read floats 8w..8w+7 of row r) fall in four distinct bank octets.
+  static constexpr int P = (PW % 16 == 0) ? PW + 8 : PW;
   static constexpr int W = T / 32;                        // warps
-  static constexpr int NWC = P / 8, NWR = (RYM + 7) / 8;  // warp tiles (8 rows x 8 floats) per row / column
+  static constexpr int NWC = PW / 8, NWR = (RYM + 7) / 8;  // warp tiles (8 rows x 8 floats) per row / column
   static constexpr int NWT = NWR * NWC;
   static constexpr int C = (NWT + W - 1) / W;             // pairs per thread (warp tiles per warp)
   static constexpr int PLANE = NWR * 8 * P;               // floats of a plane (rows rounded up to 8)
@@ -333,8 +336,13 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
         for (int c = 0; c < C; ++c) {  // dead warp tiles: zero fill past the plane, no read
           const int r = rc[c];
           const bool v0 = (am[0] >> (2 * c)) & 1u, v1 = (am[0] >> (2 * c + 1)) & 1u;
-          cp_async4(dst + r, v0 ? src + goff[c] : in, v0);
-          cp_async4(dst + r + 1, v1 ? src + goff[c] + 1 : in, v1);
+          const float* s0 = src + goff[c];
+          if (v0 && v1 && (reinterpret_cast<uintptr_t>(s0) & 7u) == 0) {
+            cp_async8(dst + r, s0);  // a whole aligned pair
+          } else {
+            cp_async4(dst + r, v0 ? s0 : in, v0);
+            cp_async4(dst + r + 1, v1 ? s0 + 1 : in, v1);
+          }
         }
       }
       asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -421,7 +429,6 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
         float* St = stage + sl0 * PS;
         const bool inx = i >= g + 2 && i <= X - g - 3;
         const uint32_t gen = inx ? ((am[0] & ~fm) | gm) : am[0];  // lanes with boundary work
-#pragma unroll
         if (allw && !gm) {
 #pragma unroll
           for (int c = 0; c < C; ++c) q[0][c][0] = *reinterpret_cast<const float2*>(St + rc[c]);
@@ -454,7 +461,6 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
         const bool xst = x >= g && x < X - g;
         const uint32_t gen = inx ? ((am[s] & ~fm) | gm) : am[s];
         if (!gen) {  // no boundary work in this thread's pairs
-#pragma unroll
           if (allw) {
 #pragma unroll
             for (int c = 0; c < C; ++c) {
@@ -503,7 +509,6 @@ __global__ void __launch_bounds__(T, (H3Cfg<R, K, N, TYM, TZM, T>::MINB))
           const bool xst = x >= g && x < X - g;
           float* orow = out + (long long)x * YZN;
           if (inx && !gm && !(am[K] & ~fm)) {  // every output lane a stencil cell
-#pragma unroll
             float2 u[C];
             if (allw) {
 #pragma unroll
