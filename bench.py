@@ -219,7 +219,10 @@ def sweep_config(world: int) -> dict:
             "interior": [N_INT, N_INT, N_INT], "ops_per_step": 6,
             "fields": "scalar (512+2g)^3 and vec3 (512+2g)^3 per order",
             "l2": "inputs larger than L2 (>=543 MB each), no flush",
-            "parallelism": f"dp{world}" if world > 1 else "single"}
+            "parallelism": f"x-slabs{world}" if world > 1 else "single",
+            **({"halo_exchange": "every step, before the operators: the g halo planes of each input field "
+                                 "from both X neighbours (periodic), NCCL send/recv into the field's own planes",
+                "global_interior": [N_INT * world, N_INT, N_INT]} if world > 1 else {})}
 
 
 def run_reference(args):
@@ -313,7 +316,17 @@ def run_ours(args):
         fast_ops.append((f"grad_o{order}", lambda u=u, grd=grd: grd(u, 1.0), ALG_BYTES["grad"]))
         fast_ops.append((f"divergence_o{order}", lambda v=v, div=div: div(v, 1.0), ALG_BYTES["divergence"]))
 
+    # N > 1: the slabs are cut along X; every step first refreshes each input
+    # field's g halo planes from the neighbouring ranks (periodic), in the timed region
+    exch = []
+    if world > 1:
+        for order in (2, 4):
+            u, v, _ = fields[order]
+            exch.append(lambda u=u, v=v, g=order // 2: (exchange_slab_halos(u, g), exchange_slab_halos(v, g)))
+
     def step():
+        for fn in exch:
+            fn()
         for _, fn, _ in ops:
             fn()
 
@@ -338,6 +351,8 @@ def run_ours(args):
     time.sleep(0.3)
     t0.record(stream)
     for k in range(K):
+        for fn in exch:
+            fn()
         for j, (_, fn, _) in enumerate(ops):
             ev[k][j][0].record(stream)
             fn()
@@ -408,8 +423,10 @@ def run_ours(args):
         e2e = run_e2e(fields, ops, world, args)
 
     heat3d = None
-    if world == 1 and not args.no_heat3d:  # a single-GPU workload (replicas only): not run beside other ranks
+    if world == 1 and not args.no_heat3d:
         heat3d = run_heat3d()
+    elif not args.no_heat3d:  # collective: every rank runs its slab
+        heat3d = run_heat3d_slabs(world, rank)
     heat = None
     if world == 1 and not args.no_heat:  # a single-GPU workload (replicas only): not run beside other ranks
         heat = run_heat()
@@ -547,6 +564,41 @@ def run_heat3d(n: int = 512, steps: int = 12, depths=(1, 2, 3, 4)):
     return out
 
 
+def run_heat3d_slabs(world: int, rank: int, n: int = 512, steps: int = 12) -> dict:
+    """3D heat on a (n*world) x n x n interior cut into X slabs of n planes, one
+    per rank (weak scaling), order 2 at the library's depth k, Dirichlet 0 on all
+    faces: each block of k steps is one halo exchange (g + k + 1 planes to each
+    neighbour, NCCL send/recv) and one fused pass.  CUDA events around `steps`
+    steps after one untimed call, the max over ranks."""
+    import torch
+    import torch.distributed as dist
+    import pde_module_b200 as P
+    from pde_module_b200.distributed import SlabHeatRollout
+    g, X = 1, n * world + 2
+    dx = 1.0 / (n - 1)
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(11 + rank)
+    bc = P.GridBoundary(torch.empty((4, n + 2, n + 2, 1), device="cuda"), dx, g)
+    bc.dirichlet_BC("ALL", 0.0)
+    roll = SlabHeatRollout(bc, dx, 1.0, 0.15 * dx * dx, X)
+    roll.owned.copy_(torch.rand(roll.owned.shape, device="cuda", generator=gen))
+    roll(steps)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    roll(steps)
+    e1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1) / steps], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    return {"workload": f"3D heat {n * world}x{n}x{n} in {world} X slabs, Dirichlet 0, order 2, exact",
+            "k": roll.k, "halo_planes": roll.halo, "ms_per_step": round(ms, 4),
+            "cell_updates_per_s": world * n ** 3 / (ms / 1000.0), "scaling": "weak",
+            "exchange": "per block of k steps, inside the timed region"}
+
+
 def leg_summary(kern, heat3d, heat, ldc, wave, batched, wc) -> dict:
     """The key figure of every leg, short (the line's last key)."""
     def g(d, *path):
@@ -556,7 +608,10 @@ def leg_summary(kern, heat3d, heat, ldc, wave, batched, wc) -> dict:
             d = d[p]
         return round(d, 4) if isinstance(d, float) else d
     out = {"sweep_frac": {k: v["frac"] for k, v in kern.items()}}
-    if heat3d:
+    if heat3d and "order2" not in heat3d:  # N > 1: the slab rollout
+        out["heat3d_slabs"] = {"k": heat3d["k"], "ms_per_step": heat3d["ms_per_step"],
+                               "gcups": round(heat3d["cell_updates_per_s"] / 1e9, 1)}
+    elif heat3d:
         out["heat3d_512"] = {f"o{o}": {"k": g(heat3d, f"order{o}", "best_k"),
                                        "ms_per_step": g(heat3d, f"order{o}", "ms_per_step"),
                                        "gcups": round(heat3d[f"order{o}"]["cell_updates_per_s"] / 1e9, 1),

@@ -256,6 +256,19 @@ int pde_heat_rollout_at(const float* u_in, float* u_out, float* work, const PdeG
                         int32_t nsteps, int32_t steps_per_pass, double t0, double t_step,
                         void* stream);
 
+/* pde_heat_rollout_at continuing a run at step n0 >= 0: step n of the call
+ * fills the boundary at fp32(t0 + (n0 + n) * t_step), so consecutive calls of
+ * k steps (n0 = 0, k, 2k, ...) equal one call of the whole run bit for bit (the
+ * slab rollout's blocks between halo exchanges). */
+int pde_heat_rollout_from(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
+                          int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
+                          int32_t nsteps, int32_t steps_per_pass, double t0, double t_step,
+                          int32_t n0, void* stream);
+
+/* Steps per pass pde_heat_rollout uses on this grid for a steps_per_pass
+ * request (0 = choose), or a negative status.  Needs no GPU. */
+int pde_heat_pass_depth(const PdeGrid* grid, int32_t ncomp, int32_t steps_per_pass);
+
 /* ---- differentiable heat rollout (new: the reference has the forward loop
  * only, examples/2D_Heat_Equation.py:57-65, with a scalar alpha) ----
  * 2D grids, one component, order 2 or 4, constant-valued face groups.

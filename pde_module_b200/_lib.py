@@ -147,6 +147,10 @@ _SIGS = {
     "pde_heat_rollout_at": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
                                       C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
                                       C.c_double, C.c_double, C.c_void_p]),
+    "pde_heat_rollout_from": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PdeGrid), C.c_int32,
+                                        C.POINTER(PdeBCRules), C.c_float, C.c_float, C.c_int32, C.c_int32,
+                                        C.c_double, C.c_double, C.c_int32, C.c_void_p]),
+    "pde_heat_pass_depth": (C.c_int, [C.POINTER(PdeGrid), C.c_int32, C.c_int32]),
     "pde_ldc_rollout": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.POINTER(PdeGrid), C.POINTER(PdeBCRules), C.POINTER(PdeBCRules),
                                   C.POINTER(PdeLDCParams), C.c_int32, C.c_void_p]),

@@ -521,11 +521,23 @@ float host_ramp_value(const PdeBCGroupParam& B, double t0, double tstep, long lo
   return r * B.value;
 }
 
-// The fused rollout; time-dependent groups only when `allow_ramp`.
+// Steps per pass of the fused rollout for a request (0 = choose): 2D grids 8;
+// 3D grids on the streaming kernel 2 for order 2 and 1 for order 4 (the
+// fastest depths at 512^3 on B200), at most heat3d_kmax; other 3D grids 1.
+int heat_depth(const Geo& G, int ncomp, int steps_per_pass) {
+  const bool two_d = (G.ndims == 2 && G.n[2] == 1);
+  if (two_d) return steps_per_pass > 0 ? steps_per_pass : 8;
+  if (!heat3d_ok(G, ncomp)) return 1;
+  const int k = steps_per_pass > 0 ? steps_per_pass : (G.order == 2 ? 2 : 1);
+  return k > heat3d_kmax(ncomp) ? heat3d_kmax(ncomp) : k;
+}
+
+// The fused rollout; time-dependent groups only when `allow_ramp`; step n of
+// the call fills the boundary at fp32(t0 + (n0 + n) * tstep).
 int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
                      const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
-                     bool allow_ramp, double t0, double tstep, void* stream) {
-  if (!u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0) return PDE_ERR_ARG;
+                     bool allow_ramp, double t0, double tstep, int32_t n0, void* stream) {
+  if (!u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0 || n0 < 0) return PDE_ERR_ARG;
   if (ncomp < 1 || ncomp > PDE_FUSED_MAX_COMP || rules->ncomp != ncomp) return PDE_ERR_ARG;
   if (rules->has_ramp && !allow_ramp) return PDE_ERR_UNSUPPORTED;
   if (rules->ngroups < 0 || rules->ngroups > PDE_MAX_GROUPS) return PDE_ERR_ARG;
@@ -543,11 +555,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
   const int R = W.radius;
   const bool two_d = (G.ndims == 2 && G.n[2] == 1);
   const bool s3d = !two_d && heat3d_ok(G, ncomp);
-  int k = two_d ? (steps_per_pass > 0 ? steps_per_pass : 8) : 1;
-  if (s3d) {
-    k = steps_per_pass > 0 ? steps_per_pass : (R == 1 ? 2 : 1);  // fastest depths at 512^3 on B200
-    if (k > heat3d_kmax(ncomp)) k = heat3d_kmax(ncomp);
-  }
+  int k = heat_depth(G, ncomp, steps_per_pass);
   if (k > nsteps) k = nsteps;
   const int npasses = (nsteps + k - 1) / k;
   // buffer sequence: the last pass writes u_out.
@@ -591,7 +599,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
       const int tiles = ((P.X + P.TBX - 1) / P.TBX) * P.tiles_y;
       for (int t = 0; t < 5; ++t) P.w[t] = W.w[t];
       P.alpha = alpha; P.dt = dt;
-      P.t0 = t0; P.tstep = tstep; P.n0 = done;
+      P.t0 = t0; P.tstep = tstep; P.n0 = n0 + done;
       const size_t smem = (size_t)2 * P.RXM * P.RYM * ncomp * sizeof(float);
       if (smem > 227 * 1024 - sizeof(PdeBCRules)) return PDE_ERR_TOO_LARGE;
       // one component and at most 8 region cells per thread: the register cell-list kernel
@@ -637,7 +645,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
 #undef PDE_H2
       }
     } else if (s3d) {
-      const int lrc = launch_heat3d(ks, R, ncomp, src, dst, G, W, alpha, dt, rules, t0, tstep, done, st);
+      const int lrc = launch_heat3d(ks, R, ncomp, src, dst, G, W, alpha, dt, rules, t0, tstep, n0 + done, st);
       if (lrc) return lrc;
     } else {
       const int64_t total = G.n[0] * G.n[1] * G.n[2] * ncomp;
@@ -645,7 +653,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
       PdeBCRules Rs = *rules;
       if (rules->has_ramp)
         for (int i = 0; i < rules->ngroups; ++i)
-          if (rules->group[i].func == PDE_BC_FUNC_RAMP) Rs.group[i].value = host_ramp_value(rules->group[i], t0, tstep, done);
+          if (rules->group[i].func == PDE_BC_FUNC_RAMP) Rs.group[i].value = host_ramp_value(rules->group[i], t0, tstep, (long long)n0 + done);
       if (R == 1) heat_step_kernel<1><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, Rs, total);
       else heat_step_kernel<2><<<grid_blocks(total, 256), 256, 0, st>>>(src, dst, G, ncomp, W, alpha, dt, Rs, total);
     }
@@ -665,14 +673,28 @@ int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid
                      const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
                      void* stream) {
   return heat_rollout_run(u_in, u_out, work, grid, ncomp, rules, alpha, dt, nsteps, steps_per_pass, false, 0.0, 0.0,
-                          stream);
+                          0, stream);
 }
 
 int pde_heat_rollout_at(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
                         const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
                         double t0, double t_step, void* stream) {
   return heat_rollout_run(u_in, u_out, work, grid, ncomp, rules, alpha, dt, nsteps, steps_per_pass, true, t0, t_step,
-                          stream);
+                          0, stream);
+}
+
+int pde_heat_rollout_from(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
+                          const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
+                          double t0, double t_step, int32_t n0, void* stream) {
+  return heat_rollout_run(u_in, u_out, work, grid, ncomp, rules, alpha, dt, nsteps, steps_per_pass, true, t0, t_step,
+                          n0, stream);
+}
+
+int pde_heat_pass_depth(const PdeGrid* grid, int32_t ncomp, int32_t steps_per_pass) {
+  if (!grid || ncomp < 1 || ncomp > PDE_FUSED_MAX_COMP || steps_per_pass < 0) return PDE_ERR_ARG;
+  Geo G;
+  if (!make_geo(grid, &G)) return PDE_ERR_SHAPE;
+  return heat_depth(G, ncomp, steps_per_pass);
 }
 
 namespace {

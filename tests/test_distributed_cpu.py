@@ -155,3 +155,126 @@ def test_slab_rows_and_local_exchange():
     exchange_local_slabs(fields, 4)
     for f, (lo, hi, hl, hh) in zip(fields, rows):
         assert torch.equal(f, glob[hl:hh])
+
+
+# ---------------------------------------------------------------- slab heat ---
+# Global 3D heat problem of the slab tests: Dirichlet 0.25 on every face, then
+# Neumann 0.5 on -Y and a Dirichlet ramp to 0.8 on +Z (t_max inside the run).
+def _slab_groups(shape, g, dt, nsteps):
+    from oracle import fdm
+    G = fdm.exterior_groups(shape, g)
+    return [dict(ids=G["ALL"], type=1, value=0.25, comps=(0,), func="constant"),
+            dict(ids=G["-Y"], type=2, value=0.5, comps=(0,), func="constant"),
+            dict(ids=G["+Z"], type=1, value=0.8, comps=(0,), func="ramp", t_max=0.5 * nsteps * dt)]
+
+
+def _slab_problem(order, X):
+    g = order // 2
+    shape = (X, 7 + 2 * g, 6 + 2 * g)
+    rng = np.random.default_rng(11)
+    u0 = rng.random(shape + (1,)).astype(np.float32)
+    dx = 1.0 / (shape[1] - 2 * g - 1)
+    return g, shape, u0, dx, 0.15 * dx * dx
+
+
+def _oracle_stepper(slab, g, order, dx, dt, nsteps_total, t0):
+    """The oracle's heat steps over the slab array, with the slab's own face groups."""
+    from oracle import fdm
+
+    def step(src, dst, nsteps, n0):
+        u = src.numpy()
+        groups = _slab_groups(u.shape[:3], g, dt, nsteps_total)
+        for n in range(nsteps):
+            u = fdm.heat_step(u, groups, dx, g, 1.0, dt, order, np.float32, t0 + (n0 + n) * dt)
+        dst.copy_(torch.from_numpy(u))
+    return step
+
+
+def _slab_reference(u0, g, order, dx, dt, nsteps, t0):
+    from oracle import fdm
+    groups = _slab_groups(u0.shape[:3], g, dt, nsteps)
+    u = u0
+    for n in range(nsteps):
+        u = fdm.heat_step(u, groups, dx, g, 1.0, dt, order, np.float32, t0 + n * dt)
+    return u
+
+
+def _make_slab(rank, world, order, k, X, nsteps, t0, local=False):
+    from pde_module_b200.FDM.boundary import GridBoundary
+    from pde_module_b200.distributed import SlabHeatRollout
+    g, shape, u0, dx, dt = _slab_problem(order, X)
+    bc = GridBoundary(torch.zeros(shape + (1,)), dx, g)
+    holder = {}
+    kw = dict(rank=rank, world=world) if local else {}
+    s = SlabHeatRollout(bc, dx, 1.0, dt, X, order=order, steps_per_pass=k, device="cpu",
+                        stepper=lambda *a: holder["f"](*a), **kw)
+    holder["f"] = _oracle_stepper(s, g, order, dx, dt, nsteps, t0)
+    s.load(torch.from_numpy(u0))
+    ref = _slab_reference(u0, g, order, dx, dt, nsteps, t0)
+    return s, ref
+
+
+def _slab_worker(rank, world, port, order, k, X, nsteps, t0, q):
+    try:
+        _init(rank, world, port)
+        s, ref = _make_slab(rank, world, order, k, X, nsteps, t0)
+        s(nsteps - 2, t0)   # two calls: the step count carries over
+        got = s(2, t0).numpy()
+        a, b = s.own
+        ok = bool(np.array_equal(got, ref[a:b]))
+        dist.barrier()
+        dist.destroy_process_group()
+        q.put((rank, ok))
+    except Exception as e:  # report instead of hanging the parent
+        q.put((rank, repr(e)))
+
+
+def test_slab_partition_and_halo():
+    from pde_module_b200.distributed import slab_partition, slab_halo
+    for X, g, world in [(516, 2, 4), (514, 1, 8), (25, 2, 3), (10, 1, 1)]:
+        parts = slab_partition(X, g, world)
+        assert parts[0][0] == 0 and parts[-1][1] == X
+        assert all(parts[i][1] == parts[i + 1][0] for i in range(world - 1))
+        sizes = [b - a for a, b in parts]
+        inner = [sizes[0] - g] + sizes[1:-1] + [sizes[-1] - g] if world > 1 else [sizes[0] - 2 * g]
+        assert max(inner) - min(inner) <= 1 and sum(inner) == X - 2 * g
+    assert slab_halo(1, 2, 2) == 4 and slab_halo(2, 4, 1) == 5
+    with pytest.raises(ValueError):
+        slab_partition(6, 2, 3)
+
+
+@pytest.mark.parametrize("world,order,k,nsteps", [(2, 2, 3, 7), (2, 4, 1, 5), (3, 4, 2, 7), (3, 2, 2, 6)])
+def test_slab_heat_rollout_equals_single_array(world, order, k, nsteps):
+    """gloo ranks, each stepping its slab (halo planes beside the cuts, exchanged
+    every k steps) with the oracle: the owned planes equal the whole-array run,
+    with Dirichlet, Neumann and ramp groups and a block that ends short."""
+    X = world * (order // 2 + k * (order // 2) + 1) + order + 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_slab_worker, args=(r, world, port, order, k, X, nsteps, 0.25, q))
+          for r in range(world)]
+    for p in ps:
+        p.start()
+    res = dict(q.get(timeout=180) for _ in range(world))
+    for p in ps:
+        p.join(timeout=60)
+    assert res == {r: True for r in range(world)}, res
+
+
+@pytest.mark.parametrize("world,order,k", [(1, 2, 2), (2, 2, 2), (4, 2, 1), (3, 4, 2)])
+def test_local_slabs_equal_single_array(world, order, k):
+    """The same decomposition with all slabs in one process (advance_local_slabs)."""
+    from pde_module_b200.distributed import advance_local_slabs
+    X = world * (order // 2 + k * (order // 2) + 1) + order + 2
+    nsteps = 2 * k + 1
+    slabs, ref = zip(*[_make_slab(r, world, order, k, X, nsteps, 0.0, local=True) for r in range(world)])
+    advance_local_slabs(list(slabs), nsteps)
+    for s in slabs:
+        a, b = s.own
+        assert np.array_equal(s.owned.numpy(), ref[0][a:b]), s.rank
+    with pytest.raises(RuntimeError):
+        if world > 1:
+            slabs[0](1)
+        else:
+            raise RuntimeError

@@ -45,6 +45,18 @@ def test_argument_validation_needs_no_gpu():
     assert L.pde_bc_compile(grp, 1, C.byref(g), 1, C.byref(r)) == _lib.PDE_ERR_UNSUPPORTED
 
 
+def test_heat_pass_depth_needs_no_gpu():
+    """The depth pde_heat_rollout runs (the slab rollout sizes its halos by it)."""
+    L = _lib.lib()
+    d = lambda shape, g, order, N, k: L.pde_heat_pass_depth(C.byref(_lib.make_grid(shape, g, order, 0.1)), N, k)
+    assert d((66, 66, 1), 1, 2, 1, 0) == 8 and d((66, 66, 1), 1, 2, 1, 5) == 5    # 2D: 8 unless asked
+    assert d((514, 514, 514), 1, 2, 1, 0) == 2 and d((516, 516, 516), 2, 4, 1, 0) == 1
+    assert d((40, 40, 40), 1, 2, 1, 9) == 4 and d((40, 40, 40), 1, 2, 3, 4) == 2  # capped per component count
+    assert d((40, 4, 40), 1, 2, 1, 3) == 1                                          # 2 interior rows: one step per pass
+    assert d((40, 40, 40), 1, 2, 0, 0) == _lib.PDE_ERR_ARG
+    assert L.pde_heat_pass_depth(None, 1, 0) == _lib.PDE_ERR_ARG
+
+
 def test_ramp_rules_compile_and_only_the_timed_rollout_takes_them():
     """A ramp group compiles with has_ramp set; pde_heat_rollout (constant groups)
     refuses such rules before touching any memory, pde_heat_rollout_at validates
