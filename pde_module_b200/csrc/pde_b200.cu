@@ -64,7 +64,7 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK, int MODE>
 int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& Wt, double alpha_d, float alpha,
                       cudaStream_t st) {
-  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK>;
+  using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>;
   auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>;
   static int occ = -1;
   if (occ < 0) {
@@ -168,19 +168,29 @@ int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt
 // Tile configurations of the streaming kernels.  Candidate 0 is the default
 // for every shape and mode; candidates 1-3 are compiled for double-row
 // addressing (even Y and Z), exact arithmetic, and are picked per
-// (operator, order) by pde_stream3d_select (the autotuner sweeps them).
+// (operator, order) by pde_stream3d_select (the autotuner sweeps them).  The
+// scalar Laplacian at order 4 runs z-pair consumers (two cells per lane), so
+// its tiles hold twice the z cells per lane of the others.
 enum { S3K_LAP1 = 0, S3K_LAP3 = 1, S3K_GRAD = 2, S3K_DIV = 3, S3K_KINDS = 4 };
 // Defaults [kind][order 2, order 4]: the fastest candidates of a sweep at 512^3 on B200.
-int g_s3_sel[S3K_KINDS][2] = {{2, 2}, {3, 3}, {3, 3}, {1, 1}};
+int g_s3_sel[S3K_KINDS][2] = {{2, 1}, {3, 3}, {3, 2}, {1, 1}};
 constexpr int kS3Candidates = 4;
 
 template <int R, int OP, int CIN>
 int launch_candidate(int cand, const float* in, float* out, const Geo& G, const Weights& W, float alpha,
                      cudaStream_t st) {
-  if constexpr (OP == OP_LAP && CIN == 1) {
+  if constexpr (OP == OP_LAP && CIN == 1 && R == 2) {  // z-pair consumers (TZ/2 lanes per row group)
+    switch (cand) {
+      case 1: return launch_stream3d_k<R, OP, 1, 128, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 2: return launch_stream3d_k<R, OP, 1, 64, 32, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 3: return launch_stream3d_k<R, OP, 1, 128, 8, 2, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      default: return launch_stream3d_k<R, OP, 1, 64, 32, 8, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+    }
+  } else if constexpr (OP == OP_LAP && CIN == 1) {
     switch (cand) {
       case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 2: return launch_stream3d_k<R, OP, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 3: return launch_stream3d_k<R, OP, 1, 128, 8, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       default: return launch_stream3d_k<R, OP, 1, 64, 32, 8, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
     }
   } else if constexpr (OP == OP_LAP) {
