@@ -56,10 +56,11 @@ enum { MODE_EXACT = 0, MODE_FAST = 1 };
 
 template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK = MAP_ROWS_PP0, int MODE = MODE_EXACT>
 struct S3Cfg {
-  // z pairs (scalar Laplacian, radius 2, double-row map, exact): a consumer lane
-  // owns two adjacent z cells, an 8-byte aligned pair in every stage row (the
-  // radius and every row lead are even), see s3_lap_zpairs
-  static constexpr bool ZP = OP == OP_LAP && CIN == 1 && R == 2 && MAPK == MAP_PAIRS && MODE == MODE_EXACT;
+  // z pairs (scalar Laplacian or Grad, radius 2, double-row map, exact): a
+  // consumer lane owns two adjacent z cells, an 8-byte aligned pair in every
+  // stage row (the radius and every row lead are even), see s3_zpairs
+  static constexpr bool ZP =
+      (OP == OP_LAP || OP == OP_GRAD) && CIN == 1 && R == 2 && MAPK == MAP_PAIRS && MODE == MODE_EXACT;
   static constexpr int LANES = ZP ? TZ / 2 : (OP == OP_LAP) ? TZ * CIN : TZ;  // consumer threads per row group
   static constexpr int TYG = TY / YPT;                           // row groups
   static constexpr int NCONS = LANES * TYG;                      // consumer threads
@@ -92,17 +93,81 @@ struct FastW {
   float a[3];  // LAP: alpha*w[t] for the off-centre taps t < R (mirror t' = T-1-t); [R]: alpha*D*w[R]
 };              // D1: alpha*w[t] for t > R (antisymmetric: w[T-1-t] = -w[t])
 
-// Consumers of the scalar Laplacian at radius 2 with z pairs (S3Cfg::ZP): lane
-// l owns the z cells z0 + 2l and z0 + 2l + 1 of YPT consecutive rows, an
+// Grad output of one plane: tile row t owns 3 TZ consecutive output floats.
+// Every consumer thread calls this once per plane after staging its results in
+// ob, row t at float (r0 + t dzr) mod 32 (the row's offset within a 128-byte
+// line of the array, whose offset of row t is rf0 + 3 Z t); the consumers meet
+// at a named barrier and store the rows.  Order 4 (BULK): one lane per row hands
+// the row's 16-byte aligned body to the bulk-copy unit (smem and global
+// offsets agree mod 16 bytes) and lanes store the head and tail floats.  Order
+// 2: every warp stores whole rows as line-aligned 128-byte pieces, one line per
+// store.  (Measured at 512^3 on B200: bulk rows 0.79 vs 0.72 of HBM at order
+// 4, 0.78 vs 0.83 at order 2.)  Two buffers: a buffer is rewritten two planes
+// later, after the next plane's barrier, before which every issuing lane has
+// waited for its bulk copies to finish reading; one buffer: a second barrier
+// (after that wait) follows the stores.
+template <class C, int R, int TZ, int TY>
+__device__ __forceinline__ void s3_grad_rows(const S3Params& P, const float* ob, size_t rf0, int r0, int dzr,
+                                             int y0, int z0) {
+  const int tid = threadIdx.x;
+  constexpr bool BULK = (R >= 2);
+  if constexpr (BULK) {
+    fence_proxy_async_smem();  // the staged rows are read by the async proxy
+    bulk_wait_read();          // this lane's bulk stores of two planes ago have read their buffer
+  }
+  asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
+  const int wl = tid & 31;
+  const int nf = 3 * min(TZ, P.Z - P.g - z0);  // floats of the row's interior cells
+  for (int t = tid >> 5; t < TY && y0 + t < P.Y - P.g; t += C::NCW) {
+    const int r = (r0 + t * dzr) & 31;  // the row's float offset in its 128-byte line
+    if constexpr (BULK) {
+      float* gr = P.out + rf0 + (size_t)t * 3 * P.Z;
+      const float* sr = ob + t * C::OROW + r;
+      const int h = min((4 - (r & 3)) & 3, nf);  // floats before the first 16-byte boundary
+      const int body = (nf - h) & ~3;            // whole 16-byte units after them
+      const int e = h + body;                    // the tail: floats e .. nf-1 (< 4)
+      if (wl < h) gr[wl] = sr[wl];
+      else if (wl >= 4 && wl - 4 < nf - e) gr[e + wl - 4] = sr[e + wl - 4];
+      if (wl == 0 && body > 0) {
+        bulk_store(gr + h, sr + h, (uint32_t)body * 4u);
+        bulk_commit();
+      }
+    } else {
+      constexpr int NL = 3 * TZ / 32 + 1;  // lines a row can touch
+      const int a = wl - r;  // float of the row this lane stores in the row's first line
+      float* gr = P.out + rf0 + (size_t)t * 3 * P.Z + a;
+      const float* sr = ob + t * C::OROW + r + a;
+      if (nf == 3 * TZ) {  // a whole row: only the first and last lines are partial
+        if (a >= 0) gr[0] = sr[0];
+#pragma unroll
+        for (int i = 1; i < NL - 1; ++i) gr[32 * i] = sr[32 * i];
+        if (a + 32 * (NL - 1) < nf) gr[32 * (NL - 1)] = sr[32 * (NL - 1)];
+      } else {
+#pragma unroll
+        for (int i = 0; i < NL; ++i)
+          if (a + 32 * i >= 0 && a + 32 * i < nf) gr[32 * i] = sr[32 * i];
+      }
+    }
+  }
+  if (C::OBUFS == 1) {
+    if constexpr (BULK) bulk_wait_read();
+    asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
+  }
+}
+
+// Consumers with z pairs (S3Cfg::ZP: scalar Laplacian or Grad at radius 2):
+// lane l owns the z cells z0 + 2l and z0 + 2l + 1 of YPT consecutive rows, an
 // aligned float2 in every stage row, so its x-queue entries, centre-plane rows
 // and z taps are 8-byte loads (the z taps of the pair, cells z-2 .. z+3, are
 // the row's pairs at -2, 0, +2 and two pairs recombined in registers) and its
 // two cells are summed as one packed pair: products __ffma2_rn with a -0
 // addend (exactly rounded), sums __fadd2_rn, in the reference order (x, y, z
 // taps low to high, alpha last), each lane the scalar kernels' operations.
-template <int R, int TZ, int TY, int YPT, int PREF>
-__device__ __forceinline__ void s3_lap_zpairs(const S3Params& P, float* smem, uint64_t* full, uint64_t* empty) {
-  using C = S3Cfg<R, OP_LAP, 1, TZ, TY, YPT, PREF, MAP_PAIRS, MODE_EXACT>;
+// Grad stages the pair's six output floats as three 8-byte stores.
+template <int R, int OP, int TZ, int TY, int YPT, int PREF>
+__device__ __forceinline__ void s3_zpairs(const S3Params& P, float* smem, uint64_t* full, uint64_t* empty,
+                                          float* obuf) {
+  using C = S3Cfg<R, OP, 1, TZ, TY, YPT, PREF, MAP_PAIRS, MODE_EXACT>;
   static_assert(R == 2 && YPT % 2 == 0, "z pairs: radius 2, even rows per thread");
   constexpr int S = C::S, T = 2 * R + 1, M = YPT + 2 * R;
   const int tid = threadIdx.x;
@@ -117,7 +182,8 @@ __device__ __forceinline__ void s3_lap_zpairs(const S3Params& P, float* smem, ui
   for (int t = 0; t < T; ++t) w2[t] = make_float2(P.w[t], P.w[t]);
   const float2 al2 = make_float2(P.alpha, P.alpha), nz2 = make_float2(P.negzero, P.negzero);
   auto M2 = [&](float2 a, float2 b) { return __ffma2_rn(a, b, nz2); };
-  const bool st2 = (reinterpret_cast<uintptr_t>(P.out) & 7u) == 0;  // pair stores need an 8-byte aligned output
+  // pair stores (Laplacian) and pair staging (Grad: even line offsets) need an 8-byte aligned output
+  const bool st2 = (reinterpret_cast<uintptr_t>(P.out) & 7u) == 0;
 
   bool dead = false;
   int ns = 0, nph = 0, cs = 0;  // newest plane's stage and parity, centre plane's stage
@@ -134,6 +200,9 @@ __device__ __forceinline__ void s3_lap_zpairs(const S3Params& P, float* smem, ui
   };
   const int nx = P.X - 2 * P.g;
   const int oplane = P.Y * P.Z;
+  int opc = 0;  // grad: planes stored so far (selects the staging buffer)
+  const int obase = (int)((reinterpret_cast<uintptr_t>(P.out) >> 2) & 31u);  // grad: out's float offset in its line
+  const int dzr = (3 * P.Z) & 31;  // grad: line offset step from one output row to the next
 
   for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
     const int c = item / P.ntiles, tile = item - c * P.ntiles;
@@ -185,32 +254,69 @@ __device__ __forceinline__ void s3_lap_zpairs(const S3Params& P, float* smem, ui
         float2 col[M];
 #pragma unroll
         for (int m = 0; m < M; ++m) col[m] = ld2(sc + rowoff(m) + off[m & 1]);
-        float2 res[YPT];
+        float2 res[YPT][(OP == OP_GRAD) ? 3 : 1];
 #pragma unroll
         for (int k = 0; k < YPT; ++k) {
           const float* rp = sc + rowoff(R + k) + off[(R + k) & 1];
           const float2 zl = ld2(rp - 2), zr = ld2(rp + 2), cc = col[k + R];
           const float2 zt[T] = {zl, make_float2(zl.y, cc.x), cc, make_float2(cc.y, zr.x), zr};
-          float2 acc = M2(w2[0], q[jj % T][k]);
+          if constexpr (OP == OP_LAP) {
+            float2 acc = M2(w2[0], q[jj % T][k]);
 #pragma unroll
-          for (int t = 1; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], q[(jj + t) % T][k]));
+            for (int t = 1; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], q[(jj + t) % T][k]));
 #pragma unroll
-          for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], col[k + t]));
+            for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], col[k + t]));
 #pragma unroll
-          for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], zt[t]));
-          res[k] = M2(al2, acc);
+            for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], zt[t]));
+            res[k][0] = M2(al2, acc);
+          } else {
+            float2 ax = M2(w2[0], q[jj % T][k]), ay = M2(w2[0], col[k]), az = M2(w2[0], zt[0]);
+#pragma unroll
+            for (int t = 1; t < T; ++t) {
+              ax = __fadd2_rn(ax, M2(w2[t], q[(jj + t) % T][k]));
+              ay = __fadd2_rn(ay, M2(w2[t], col[k + t]));
+              az = __fadd2_rn(az, M2(w2[t], zt[t]));
+            }
+            res[k][0] = M2(al2, ax);
+            res[k][1] = M2(al2, ay);
+            res[k][2] = M2(al2, az);
+          }
         }
-        release(cs);  // the centre plane is not read again
-        adv(cs);
-        float* op = optr + (size_t)j * oplane;
-        if (all_rows) {
-#pragma unroll
-          for (int k = 0; k < YPT; ++k) *reinterpret_cast<float2*>(op + (size_t)k * P.Z) = res[k];
-        } else {
+        if constexpr (OP == OP_GRAD) {
+          // stage: the pair's floats 3z .. 3z+5 (x, y, z of each cell) at the row's line offset
+          float* ob = obuf + (C::OBUFS == 2 ? (opc & 1) * (TY * C::OROW) : 0);
+          const size_t rf0 = (((size_t)(xs + j) * P.Y + y0) * P.Z + z0) * 3;
+          const int r0 = (obase + (int)(rf0 & 31u)) & 31;
 #pragma unroll
           for (int k = 0; k < YPT; ++k) {
-            if ((vm0 >> k) & 1u) op[(size_t)k * P.Z] = res[k].x;
-            if ((vm1 >> k) & 1u) op[(size_t)k * P.Z + 1] = res[k].y;
+            const int t = row0 + k;
+            float* sr = ob + t * C::OROW + ((r0 + t * dzr) & 31) + 6 * lane;
+            if (st2) {  // even line offset: 8-byte stores
+              *reinterpret_cast<float2*>(sr) = make_float2(res[k][0].x, res[k][1].x);
+              *reinterpret_cast<float2*>(sr + 2) = make_float2(res[k][2].x, res[k][0].y);
+              *reinterpret_cast<float2*>(sr + 4) = make_float2(res[k][1].y, res[k][2].y);
+            } else {
+              sr[0] = res[k][0].x; sr[1] = res[k][1].x; sr[2] = res[k][2].x;
+              sr[3] = res[k][0].y; sr[4] = res[k][1].y; sr[5] = res[k][2].y;
+            }
+          }
+          release(cs);  // the centre plane is not read again
+          adv(cs);
+          ++opc;
+          s3_grad_rows<C, R, TZ, TY>(P, ob, rf0, r0, dzr, y0, z0);
+        } else {
+          release(cs);  // the centre plane is not read again
+          adv(cs);
+          float* op = optr + (size_t)j * oplane;
+          if (all_rows) {
+#pragma unroll
+            for (int k = 0; k < YPT; ++k) *reinterpret_cast<float2*>(op + (size_t)k * P.Z) = res[k][0];
+          } else {
+#pragma unroll
+            for (int k = 0; k < YPT; ++k) {
+              if ((vm0 >> k) & 1u) op[(size_t)k * P.Z] = res[k][0].x;
+              if ((vm1 >> k) & 1u) op[(size_t)k * P.Z + 1] = res[k][0].y;
+            }
           }
         }
       });
@@ -222,6 +328,7 @@ __device__ __forceinline__ void s3_lap_zpairs(const S3Params& P, float* smem, ui
       adv(cs);
     }
   }
+  if constexpr (OP == OP_GRAD) bulk_wait();  // this lane's bulk stores are done before the block exits
 }
 
 // Work items are (chunk of planes, tile) pairs in chunk-major order, dealt
@@ -294,7 +401,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
 
   // ---------------- consumer threads ----------------
   if constexpr (C::ZP) {
-    s3_lap_zpairs<R, TZ, TY, YPT, PREF>(P, smem, full, empty);
+    s3_zpairs<R, OP, TZ, TY, YPT, PREF>(P, smem, full, empty, obuf);
   } else {
     const int lane = tid % C::LANES, yg = tid / C::LANES;
     const bool warp_leader = (tid & 31) == 0;
@@ -526,62 +633,8 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
           adv(cs);
           [[maybe_unused]] float* op = optr + j * oplane;  // this thread's first output (LAP, DIV)
           if constexpr (OP == OP_GRAD) {
-            // A tile row owns 3 TZ consecutive output floats (TZ / 32 warps compute
-            // it).  The consumers stage the plane's rows in shared memory, each at its
-            // global offset within a 128-byte line, and meet at a named barrier.
-            // Order 4 (BULK): one lane per row hands the row's 16-byte aligned body to
-            // the bulk-copy unit (smem and global offsets agree mod 16 bytes) and lanes
-            // store the head and tail floats.  Order 2: every warp stores whole rows
-            // as line-aligned 128-byte pieces, one line per store.  (Measured at 512^3
-            // on B200: bulk rows 0.79 vs 0.72 of HBM at order 4, 0.78 vs 0.83 at
-            // order 2.)  Two buffers: a buffer is rewritten two planes later, after the
-            // next plane's barrier, before which every issuing lane has waited for its
-            // bulk copies to finish reading; one buffer: a second barrier (after that
-            // wait) follows the stores.
-            constexpr bool BULK = (R >= 2);
             ++opc;
-            if constexpr (BULK) {
-              fence_proxy_async_smem();  // the staged rows are read by the async proxy
-              bulk_wait_read();          // this lane's bulk stores of two planes ago have read their buffer
-            }
-            asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
-            const int wl = tid & 31;
-            const int nf = 3 * min(TZ, P.Z - P.g - z0);  // floats of the row's interior cells
-            for (int t = tid >> 5; t < TY && y0 + t < P.Y - P.g; t += C::NCW) {
-              const int r = (r0 + t * dzr) & 31;  // the row's float offset in its 128-byte line
-              if constexpr (BULK) {
-                float* gr = P.out + rf0 + (size_t)t * 3 * P.Z;
-                const float* sr = ob + t * C::OROW + r;
-                const int h = min((4 - (r & 3)) & 3, nf);  // floats before the first 16-byte boundary
-                const int body = (nf - h) & ~3;            // whole 16-byte units after them
-                const int e = h + body;                    // the tail: floats e .. nf-1 (< 4)
-                if (wl < h) gr[wl] = sr[wl];
-                else if (wl >= 4 && wl - 4 < nf - e) gr[e + wl - 4] = sr[e + wl - 4];
-                if (wl == 0 && body > 0) {
-                  bulk_store(gr + h, sr + h, (uint32_t)body * 4u);
-                  bulk_commit();
-                }
-              } else {
-                constexpr int NL = 3 * TZ / 32 + 1;  // lines a row can touch
-                const int a = wl - r;  // float of the row this lane stores in the row's first line
-                float* gr = P.out + rf0 + (size_t)t * 3 * P.Z + a;
-                const float* sr = ob + t * C::OROW + r + a;
-                if (nf == 3 * TZ) {  // a whole row: only the first and last lines are partial
-                  if (a >= 0) gr[0] = sr[0];
-#pragma unroll
-                  for (int i = 1; i < NL - 1; ++i) gr[32 * i] = sr[32 * i];
-                  if (a + 32 * (NL - 1) < nf) gr[32 * (NL - 1)] = sr[32 * (NL - 1)];
-                } else {
-#pragma unroll
-                  for (int i = 0; i < NL; ++i)
-                    if (a + 32 * i >= 0 && a + 32 * i < nf) gr[32 * i] = sr[32 * i];
-                }
-              }
-            }
-            if (C::OBUFS == 1) {
-              if constexpr (BULK) bulk_wait_read();
-              asm volatile("bar.sync 1, %0;" ::"r"(C::NCONS) : "memory");
-            }
+            s3_grad_rows<C, R, TZ, TY>(P, ob, rf0, r0, dzr, y0, z0);
           } else if (all_rows) {
 #pragma unroll
             for (int k = 0; k < YPT; ++k) op[k * orow] = res[k][0];
