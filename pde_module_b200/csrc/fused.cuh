@@ -93,6 +93,87 @@ struct GlobalAcc {
   }
 };
 
+// Cells of a box shell: the cells of [b, n-b)^3 with some coordinate in the
+// t layers at either end of its axis ([b, b+t) or [n-b-t, n-b)).  Block (a, s)
+// holds the layers of axis a on side s; axes before a range over their inner
+// part [b+t, n-b-t) (their layers are earlier blocks), axes after a over
+// [b, n-b), so every shell cell is in exactly one block.  Flat index ->
+// (block, layer, the two other coordinates) with two integer divisions.
+struct Shell {
+  int n[3];
+  int b, t;
+  long long off[7];  // block (a, s) = 2a + s starts at off[2a + s]; off[6] = cells
+  __host__ __device__ void init(const int* nn, int b_, int t_) {
+    b = b_;
+    t = t_;
+    n[0] = nn[0]; n[1] = nn[1]; n[2] = nn[2];
+    off[0] = 0;
+    for (int a = 0; a < 3; ++a) {
+      long long m = t;
+      for (int q = 0; q < 3; ++q)
+        if (q != a) m *= (q < a) ? (n[q] - 2 * b - 2 * t) : (n[q] - 2 * b);
+      if (m < 0) m = 0;
+      off[2 * a + 1] = off[2 * a] + m;
+      off[2 * a + 2] = off[2 * a + 1] + m;
+    }
+  }
+  __device__ void cell(long long i, int* c) const {
+    int blk = 0;
+    while (blk < 5 && i >= off[blk + 1]) ++blk;
+    const int a = blk >> 1, s = blk & 1;
+    long long r = i - off[blk];
+    const int q0 = a == 0 ? 1 : 0, q1 = a == 2 ? 1 : 2;  // the other axes, ascending
+    const int lo0 = (q0 < a) ? b + t : b, len0 = (q0 < a) ? n[q0] - 2 * b - 2 * t : n[q0] - 2 * b;
+    const int lo1 = (q1 < a) ? b + t : b, len1 = (q1 < a) ? n[q1] - 2 * b - 2 * t : n[q1] - 2 * b;
+    const long long per_layer = (long long)len0 * len1;
+    const int l = (int)(r / per_layer);
+    r -= (long long)l * per_layer;
+    const int u = (int)(r / len1);
+    c[a] = s ? n[a] - 1 - b - l : b + l;
+    c[q0] = lo0 + u;
+    c[q1] = lo1 + (int)(r - (long long)u * len1);
+  }
+};
+
+// Surface fill of the one-step 3D heat rollout, first pass: every cell outside
+// the stencil box [g, n-g)^3 takes its boundary-filled value u2 (bc_eval) in u
+// (in place: a ghost's value reads its partner two cells inward, never another
+// ghost cell, and deeper ghosts keep their value) and in the step's output.
+__global__ void __launch_bounds__(256) heat_fill_ghosts_kernel(float* __restrict__ u, float* __restrict__ out, Geo G,
+                                                               int N, const PdeBCRules Rl, Shell S) {
+  GlobalAcc U{u, G.cstride[0], G.cstride[1], N};
+  const long long total = S.off[6] * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t / N;
+    const int v = (int)(t - i * N);
+    int c[3];
+    S.cell(i, c);
+    const float u2 = bc_eval(G, Rl, U, c[0], c[1], c[2], v);
+    const long long k = ((long long)c[0] * G.n[1] + c[1]) * G.n[2] + c[2];
+    u[k * N + v] = u2;
+    out[k * N + v] = u2;
+  }
+}
+
+// Second pass: the node layers (coordinate g or n-1-g inside the stencil box)
+// take their Dirichlet values in u, after every ghost has read its partner's
+// pre-boundary value.
+__global__ void __launch_bounds__(256) heat_fill_nodes_kernel(float* __restrict__ u, Geo G, int N,
+                                                              const PdeBCRules Rl, Shell S) {
+  GlobalAcc U{u, G.cstride[0], G.cstride[1], N};
+  const long long total = S.off[6] * N;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const long long i = t / N;
+    const int v = (int)(t - i * N);
+    int c[3];
+    S.cell(i, c);
+    const float u2 = bc_eval(G, Rl, U, c[0], c[1], c[2], v);
+    u[(((long long)c[0] * G.n[1] + c[1]) * G.n[2] + c[2]) * N + v] = u2;
+  }
+}
+
 // One fused step over the whole array (any number of eligible axes), thread
 // per (cell, component): stencil cells get u2 + dt*(alpha*L(u2)); every other
 // cell gets u2 (its boundary-filled value).

@@ -63,7 +63,7 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 // ---- 3D streaming dispatch -------------------------------------------------
 template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK, int MODE>
 int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& Wt, double alpha_d, float alpha,
-                      cudaStream_t st) {
+                      cudaStream_t st, float dt = 0.0f) {
   using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>;
   auto kern = stream3d_kernel<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>;
   static int occ = -1;
@@ -84,6 +84,7 @@ int launch_stream3d_k(const float* in, float* out, const Geo& G, const Weights& 
   P.pr = (int)((G.n[2] * CIN) & 3);
   for (int t = 0; t < 5; ++t) P.w[t] = Wt.w[t];
   P.alpha = alpha;
+  P.dt = dt;
   P.out = out;
   P.wait_ns = g_wait_ns;
   P.negzero = -0.0f;
@@ -538,15 +539,79 @@ float host_ramp_value(const PdeBCGroupParam& B, double t0, double tstep, long lo
   return r * B.value;
 }
 
+// One step per pass on the TMA streaming kernel (OP_HEAT) after a surface fill:
+// scalar 3D fields whose shape takes the double-row map (even Y and Z, 16-byte
+// plane pitch, even g - R) and whose index fits the 1D view.
+bool heat_split_shape(const Geo& G, int ncomp) {
+  if (g_dispatch == PDE_DISPATCH_GENERIC || G.ndims != 3 || ncomp != 1) return false;
+  const int R = G.order / 2;
+  const int64_t slack = 64LL * G.n[2] + 1024;
+  return pick_map<1>(G, R) == MAP_PAIRS && G.n[0] * G.n[1] * G.n[2] + slack < (1LL << 31) && G.g >= R &&
+         G.ext[0] >= 3 && G.ext[1] >= 3 && G.ext[2] >= 3;
+}
+
 // Steps per pass of the fused rollout for a request (0 = choose): 2D grids 8;
-// 3D grids on the streaming kernel 2 for order 2 and 1 for order 4 (the
-// fastest depths at 512^3 on B200), at most heat3d_kmax; other 3D grids 1.
+// 3D grids 1 where the one-step streaming path applies, else 2 for order 2 and 1
+// for order 4 on the temporally blocked kernel (the fastest depths at 512^3 on
+// B200), at most heat3d_kmax; other 3D grids 1.
 int heat_depth(const Geo& G, int ncomp, int steps_per_pass) {
   const bool two_d = (G.ndims == 2 && G.n[2] == 1);
   if (two_d) return steps_per_pass > 0 ? steps_per_pass : 8;
   if (!heat3d_ok(G, ncomp)) return 1;
-  const int k = steps_per_pass > 0 ? steps_per_pass : (G.order == 2 ? 2 : 1);
+  const int k = steps_per_pass > 0 ? steps_per_pass : (heat_split_shape(G, ncomp) ? 1 : (G.order == 2 ? 2 : 1));
   return k > heat3d_kmax(ncomp) ? heat3d_kmax(ncomp) : k;
+}
+
+// The one-step streaming 3D rollout: per step a surface fill of the source
+// buffer (ghosts into the source and the output, then nodes into the source)
+// and the OP_HEAT streaming kernel over the stencil box.  The caller's input is
+// first copied into a buffer of this call (the fill writes in place), chosen so
+// the last step lands in u_out; with u_out == u_in the rollout runs in place.
+int heat3d_split_run(const float* u_in, float* u_out, float* work, const Geo& G, const Weights& W,
+                     const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, double t0, double tstep,
+                     int32_t n0, cudaStream_t st) {
+  const size_t bytes = (size_t)(G.n[0] * G.n[1] * G.n[2]) * sizeof(float);
+  float* src;
+  float* dst;
+  if (u_out == u_in) {
+    src = u_out;
+    dst = work;
+  } else {
+    float* first = (nsteps & 1) ? work : u_out;
+    PDE_CUDA_CHECK(cudaMemcpyAsync(first, u_in, bytes, cudaMemcpyDeviceToDevice, st));
+    src = first;
+    dst = (first == work) ? u_out : work;
+  }
+  const int n[3] = {(int)G.n[0], (int)G.n[1], (int)G.n[2]};
+  Shell gs, ns;
+  gs.init(n, 0, G.g);
+  ns.init(n, G.g, 1);
+  const int sms = sm_count();
+  auto blocks_for = [&](long long cells) {
+    const long long b = (cells + 255) / 256;
+    return (int)(b < 8LL * sms ? (b > 0 ? b : 1) : 8LL * sms);
+  };
+  PdeBCRules Rs = *rules;
+  for (int s = 0; s < nsteps; ++s) {
+    if (rules->has_ramp)
+      for (int i = 0; i < rules->ngroups; ++i)
+        if (rules->group[i].func == PDE_BC_FUNC_RAMP)
+          Rs.group[i].value = host_ramp_value(rules->group[i], t0, tstep, (long long)n0 + s);
+    heat_fill_ghosts_kernel<<<blocks_for(gs.off[6]), 256, 0, st>>>(src, dst, G, 1, Rs, gs);
+    heat_fill_nodes_kernel<<<blocks_for(ns.off[6]), 256, 0, st>>>(src, G, 1, Rs, ns);
+    int rc = launch_status();
+    if (rc) return rc;
+    if (G.order == 2)
+      rc = launch_stream3d_k<1, OP_HEAT, 1, 128, 16, 8, 3, MAP_PAIRS, MODE_EXACT>(src, dst, G, W, alpha, alpha, st, dt);
+    else
+      rc = launch_stream3d_k<2, OP_HEAT, 1, 128, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(src, dst, G, W, alpha, alpha, st, dt);
+    if (rc) return rc;
+    float* t = src;
+    src = dst;
+    dst = t;
+  }
+  if (src != u_out) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, src, bytes, cudaMemcpyDeviceToDevice, st));
+  return PDE_OK;
 }
 
 // The fused rollout; time-dependent groups only when `allow_ramp`; step n of
@@ -574,6 +639,8 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
   const bool s3d = !two_d && heat3d_ok(G, ncomp);
   int k = heat_depth(G, ncomp, steps_per_pass);
   if (k > nsteps) k = nsteps;
+  if (s3d && k == 1 && heat_split_shape(G, ncomp) && aligned16(u_in) && aligned16(u_out) && aligned16(work))
+    return heat3d_split_run(u_in, u_out, work, G, W, rules, alpha, dt, nsteps, t0, tstep, n0, st);
   const int npasses = (nsteps + k - 1) / k;
   // buffer sequence: the last pass writes u_out.
   const float* src = u_in;

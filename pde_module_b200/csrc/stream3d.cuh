@@ -24,7 +24,9 @@
 
 namespace pde {
 
-enum { OP_LAP = 0, OP_GRAD = 1, OP_DIV = 2 };
+// OP_HEAT: the heat step of a boundary-filled scalar field, u2 + dt*(alpha*L(u2)),
+// on the Laplacian's tiles (exact arithmetic only)
+enum { OP_LAP = 0, OP_GRAD = 1, OP_DIV = 2, OP_HEAT = 3 };
 
 struct S3Params {
   int X, Y, Z, g;
@@ -34,6 +36,7 @@ struct S3Params {
   int pp, pr;           // (Y*Z*CIN) mod 4, (Z*CIN) mod 4: row alignment lead
   float w[5];
   float alpha;
+  float dt;             // OP_HEAT: the Euler step
   float* out;
   uint64_t wait_ns;     // bound of every mbarrier wait
   float negzero;        // -0.0f: the addend of the packed products (not a compile-time constant)
@@ -59,9 +62,10 @@ struct S3Cfg {
   // z pairs (scalar Laplacian or Grad, radius 2, double-row map, exact): a
   // consumer lane owns two adjacent z cells, an 8-byte aligned pair in every
   // stage row (the radius and every row lead are even), see s3_zpairs
+  static constexpr bool LAPL = OP == OP_LAP || OP == OP_HEAT;  // Laplacian-shaped: one output per input float
   static constexpr bool ZP =
-      (OP == OP_LAP || OP == OP_GRAD) && CIN == 1 && R == 2 && MAPK == MAP_PAIRS && MODE == MODE_EXACT;
-  static constexpr int LANES = ZP ? TZ / 2 : (OP == OP_LAP) ? TZ * CIN : TZ;  // consumer threads per row group
+      (LAPL || OP == OP_GRAD) && CIN == 1 && R == 2 && MAPK == MAP_PAIRS && MODE == MODE_EXACT;
+  static constexpr int LANES = ZP ? TZ / 2 : LAPL ? TZ * CIN : TZ;  // consumer threads per row group
   static constexpr int TYG = TY / YPT;                           // row groups
   static constexpr int NCONS = LANES * TYG;                      // consumer threads
   static constexpr int NCW = NCONS / 32;                         // consumer warps
@@ -87,6 +91,7 @@ struct S3Cfg {
   static_assert(W <= 256, "TMA box extent");
   static_assert(TY % YPT == 0, "rows per thread");
   static_assert(!ZP || TZ % 2 == 0, "z pairs");
+  static_assert(OP != OP_HEAT || (CIN == 1 && MODE == MODE_EXACT), "heat step: scalar, exact");
 };
 
 struct FastW {
@@ -181,6 +186,7 @@ __device__ __forceinline__ void s3_zpairs(const S3Params& P, float* smem, uint64
 #pragma unroll
   for (int t = 0; t < T; ++t) w2[t] = make_float2(P.w[t], P.w[t]);
   const float2 al2 = make_float2(P.alpha, P.alpha), nz2 = make_float2(P.negzero, P.negzero);
+  const float2 dt2 = make_float2(P.dt, P.dt);
   auto M2 = [&](float2 a, float2 b) { return __ffma2_rn(a, b, nz2); };
   // pair stores (Laplacian) and pair staging (Grad: even line offsets) need an 8-byte aligned output
   const bool st2 = (reinterpret_cast<uintptr_t>(P.out) & 7u) == 0;
@@ -260,7 +266,7 @@ __device__ __forceinline__ void s3_zpairs(const S3Params& P, float* smem, uint64
           const float* rp = sc + rowoff(R + k) + off[(R + k) & 1];
           const float2 zl = ld2(rp - 2), zr = ld2(rp + 2), cc = col[k + R];
           const float2 zt[T] = {zl, make_float2(zl.y, cc.x), cc, make_float2(cc.y, zr.x), zr};
-          if constexpr (OP == OP_LAP) {
+          if constexpr (C::LAPL) {
             float2 acc = M2(w2[0], q[jj % T][k]);
 #pragma unroll
             for (int t = 1; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], q[(jj + t) % T][k]));
@@ -269,6 +275,7 @@ __device__ __forceinline__ void s3_zpairs(const S3Params& P, float* smem, uint64
 #pragma unroll
             for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], zt[t]));
             res[k][0] = M2(al2, acc);
+            if constexpr (OP == OP_HEAT) res[k][0] = __fadd2_rn(cc, M2(dt2, res[k][0]));  // u2 + dt*(alpha*L)
           } else {
             float2 ax = M2(w2[0], q[jj % T][k]), ay = M2(w2[0], col[k]), az = M2(w2[0], zt[0]);
 #pragma unroll
@@ -405,7 +412,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
   } else {
     const int lane = tid % C::LANES, yg = tid / C::LANES;
     const bool warp_leader = (tid & 31) == 0;
-    const int cofs = (OP == OP_LAP) ? (R * CIN + lane) : ((R + lane) * CIN);
+    const int cofs = C::LAPL ? (R * CIN + lane) : ((R + lane) * CIN);
     constexpr int qc = 0;                         // x taps: component 0 (DIV: u_x)
     constexpr int yc = (OP == OP_DIV) ? 1 : 0;    // y taps: DIV reads u_y
     constexpr int zcmp = (OP == OP_DIV) ? 2 : 0;  // z taps: DIV reads u_z
@@ -450,8 +457,8 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
     const int dzr = (3 * P.Z) & 31;  // grad: line offset step from one output row to the next
 
     const int zrow = P.Z * CIN;
-    const int oplane = (OP == OP_LAP) ? P.Y * zrow : P.Y * P.Z * ((OP == OP_GRAD) ? 3 : 1);
-    const int orow = (OP == OP_LAP) ? zrow : P.Z * ((OP == OP_GRAD) ? 3 : 1);
+    const int oplane = C::LAPL ? P.Y * zrow : P.Y * P.Z * ((OP == OP_GRAD) ? 3 : 1);
+    const int orow = C::LAPL ? zrow : P.Z * ((OP == OP_GRAD) ? 3 : 1);
 
     for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
       const int c = item / P.ntiles, tile = item - c * P.ntiles;
@@ -478,12 +485,12 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
       if constexpr (PP0) offsets(0);
 
       unsigned vmask = 0;
-      const int zcell = (OP == OP_LAP) ? (z0 + lane / CIN) : (z0 + lane);
+      const int zcell = C::LAPL ? (z0 + lane / CIN) : (z0 + lane);
 #pragma unroll
       for (int k = 0; k < YPT; ++k)
         if (y0 + row0 + k < P.Y - P.g && zcell < P.Z - P.g) vmask |= 1u << k;
       const bool all_rows = vmask == (1u << YPT) - 1u;
-      float* optr = P.out + ((OP == OP_LAP) ? ((xs * P.Y + y0 + row0) * zrow + z0 * CIN + lane)
+      float* optr = P.out + (C::LAPL ? ((xs * P.Y + y0 + row0) * zrow + z0 * CIN + lane)
                                             : ((xs * P.Y + y0 + row0) * P.Z + zcell) * ((OP == OP_GRAD) ? 3 : 1));
 
       // x-queue: plane p (item-relative) lives in slot p % T
@@ -548,7 +555,7 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
                 return make_float2(rp0[(t - R) * zstep], rp1[(t - R) * zstep]);
               };
               auto M2 = [&](float2 a, float2 b) { return __ffma2_rn(a, b, nz2); };
-              if constexpr (OP == OP_LAP || OP == OP_DIV) {
+              if constexpr (C::LAPL || OP == OP_DIV) {
                 float2 acc = M2(w2[0], X2(0));
 #pragma unroll
                 for (int t = 1; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], X2(t)));
@@ -556,7 +563,9 @@ __global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MOD
                 for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], Y2(t)));
 #pragma unroll
                 for (int t = 0; t < T; ++t) acc = __fadd2_rn(acc, M2(w2[t], Z2(t)));
-                const float2 r = M2(al2, acc);
+                float2 r = M2(al2, acc);
+                if constexpr (OP == OP_HEAT)  // u2 + dt*(alpha*L), the centre of each row
+                  r = __fadd2_rn(make_float2(col[kp + R], col[kp + 1 + R]), M2(make_float2(P.dt, P.dt), r));
                 res[kp][0] = r.x;
                 res[kp + 1][0] = r.y;
               } else {

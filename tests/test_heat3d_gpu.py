@@ -141,3 +141,64 @@ def test_heat3d_matches_single_step_kernel(order, g, N):
     _lib.lib().pde_set_dispatch(0)
     for o in outs[1:]:
         assert torch.equal(o, outs[0])
+
+
+# Grids that take the double-row map (even Y and Z, plane pitch a multiple of 4
+# floats, even g - R): one step per pass runs the surface fill (ghosts, then
+# nodes) and the TMA streaming heat step.
+SPLIT = [
+    # shape, g, order, spec, nsteps, steps_per_pass (0: the library's choice, 1 here)
+    ((40, 38, 44), 1, 2, DIR, 7, 1),
+    ((41, 36, 40), 1, 2, MIX, 6, 0),
+    ((44, 40, 44), 2, 4, MIX, 5, 1),
+    ((39, 34, 42), 2, 4, NEU, 6, 0),
+    ((45, 40, 36), 1, 2, RAMP, 8, 1),
+    ((45, 40, 36), 2, 4, RAMP, 7, 0),
+    ((70, 150, 264), 1, 2, MIX, 5, 0),
+    ((66, 132, 260), 2, 4, MIX, 4, 0),
+]
+
+
+@pytest.mark.parametrize("shape,g,order,spec,nsteps,k", SPLIT)
+def test_heat3d_one_step_streaming(shape, g, order, spec, nsteps, k):
+    rng = np.random.default_rng(hash((shape, g, order, nsteps, k)) % (2 ** 32))
+    dx = 1.0 / (shape[0] - 2 * g - 1)
+    alpha = 0.8
+    dt = 0.15 * dx * dx / alpha
+    u0 = rng.random(shape + (1,)).astype(np.float32)
+    ud = torch.from_numpy(u0).cuda()
+    bc = _boundary(ud, dx, g, spec, nsteps, dt)
+    roll = P.HeatRollout(bc, dx, alpha, dt, order=order, steps_per_pass=k)
+    assert _lib.lib().pde_heat_pass_depth(C.byref(roll.grid), 1, k) == 1
+    t0 = 3 * dt if roll.rules.has_ramp else 0.0
+    got = roll(ud, nsteps, t0).cpu().numpy()
+    assert np.array_equal(ud.cpu().numpy(), u0)  # the input is not written
+    groups = _groups(shape, g, spec, nsteps, dt)
+    ref = fdm.heat_rollout(u0, groups, dx, g, alpha, dt, nsteps, order, t0=t0)
+    bad = np.argwhere(got != ref)
+    assert bad.size == 0, f"{len(bad)} cells differ, first {bad[:5].tolist()}"
+
+
+@pytest.mark.parametrize("nsteps", [1, 4, 5])
+def test_heat3d_one_step_streaming_in_place_and_against_blocked(nsteps):
+    """In place and out of place, odd and even step counts; equal to the
+    temporally blocked kernel at k = 2 and to the one-step generic kernel."""
+    shape, g = (52, 46, 44), 1
+    dx = 1.0 / 50
+    dt = 0.15 * dx * dx
+    rng = np.random.default_rng(17 + nsteps)
+    ud = torch.from_numpy(rng.random(shape + (1,)).astype(np.float32)).cuda()
+    bc = _boundary(ud, dx, g, MIX, 1, 1.0)
+    one = P.HeatRollout(bc, dx, 1.0, dt, steps_per_pass=1)
+    out = one(ud, nsteps).clone()
+    x = ud.clone()
+    rc = _lib.lib().pde_heat_rollout(x.data_ptr(), x.data_ptr(), one.work.data_ptr(), C.byref(one.grid), 1,
+                                     C.byref(one.rules), 1.0, dt, nsteps, 1, None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert torch.equal(x, out)
+    blocked = P.HeatRollout(bc, dx, 1.0, dt, steps_per_pass=2)(ud, nsteps).clone()
+    assert torch.equal(blocked, out)
+    _lib.lib().pde_set_dispatch(1)
+    generic = P.HeatRollout(bc, dx, 1.0, dt)(ud, nsteps).clone()
+    assert torch.equal(generic, out)

@@ -50,7 +50,9 @@ def test_heat_pass_depth_needs_no_gpu():
     L = _lib.lib()
     d = lambda shape, g, order, N, k: L.pde_heat_pass_depth(C.byref(_lib.make_grid(shape, g, order, 0.1)), N, k)
     assert d((66, 66, 1), 1, 2, 1, 0) == 8 and d((66, 66, 1), 1, 2, 1, 5) == 5    # 2D: 8 unless asked
-    assert d((514, 514, 514), 1, 2, 1, 0) == 2 and d((516, 516, 516), 2, 4, 1, 0) == 1
+    # 3D: 1 where the one-step streaming path applies (even Y and Z), else 2 (order 2) / 1 (order 4)
+    assert d((514, 514, 514), 1, 2, 1, 0) == 1 and d((516, 516, 516), 2, 4, 1, 0) == 1
+    assert d((514, 513, 514), 1, 2, 1, 0) == 2 and d((516, 515, 516), 2, 4, 1, 0) == 1
     assert d((40, 40, 40), 1, 2, 1, 9) == 4 and d((40, 40, 40), 1, 2, 3, 4) == 2  # capped per component count
     assert d((40, 4, 40), 1, 2, 1, 3) == 1                                          # 2 interior rows: one step per pass
     assert d((40, 40, 40), 1, 2, 0, 0) == _lib.PDE_ERR_ARG

@@ -43,6 +43,9 @@ CASES = [
     ((50, 21, 18), 2, 2, 4, 2, 6, False),
     ((52, 22, 19), 4, 3, 2, 2, 5, True),
     ((45, 20, 26), 2, 1, 1, 3, 7, False),
+    # even Y and Z: one step per pass on the streaming kernel after the surface fill
+    ((60, 38, 44), 2, 1, 3, 0, 7, True),
+    ((64, 36, 40), 4, 1, 2, 0, 5, False),
 ]
 
 
@@ -71,9 +74,12 @@ def test_slabs_equal_whole_array(shape, order, N, world, k, nsteps, ramp):
 
 def test_slab_halo_follows_the_pass_depth():
     """The halo is g + k*R + 1 for the depth the library runs (deeper requests
-    are capped: two components run at most 2 steps per pass)."""
+    are capped: two components run at most 2 steps per pass; a scalar field
+    with even Y and Z runs one step per pass by default)."""
     u, dx, boundary = _problem((40, 20, 20), 1, 2, 0.0, 1)
     s = SlabHeatRollout(boundary(u), dx, 1.0, 0.1 * dx * dx, 40, steps_per_pass=4, rank=0, world=2)
     assert s.k == 2 and s.halo == 1 + 2 + 1
     s = SlabHeatRollout(boundary(u[..., :1]), dx, 1.0, 0.1 * dx * dx, 40, steps_per_pass=0, rank=1, world=2)
-    assert s.k == 2 and s.h_lo == 4 and s.h_hi == 0
+    assert s.k == 1 and s.h_lo == 3 and s.h_hi == 0
+    s = SlabHeatRollout(boundary(u[:, :19, :19, :1]), dx, 1.0, 0.1 * dx * dx, 40, steps_per_pass=0, rank=0, world=2)
+    assert s.k == 2 and s.h_lo == 0 and s.h_hi == 4
