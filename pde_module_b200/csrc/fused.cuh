@@ -138,7 +138,10 @@ struct Shell {
 // Surface fill of the one-step 3D heat rollout, first pass: every cell outside
 // the stencil box [g, n-g)^3 takes its boundary-filled value u2 (bc_eval) in u
 // (in place: a ghost's value reads its partner two cells inward, never another
-// ghost cell, and deeper ghosts keep their value) and in the step's output.
+// ghost cell, and deeper ghosts keep their value) and, when out is set, in the
+// step's output (the first step seeds the constant deeper ghosts there; the last
+// leaves the result's ghosts; steps between skip it, their output's ghosts
+// being recomputed before anything reads them).
 __global__ void __launch_bounds__(256) heat_fill_ghosts_kernel(float* __restrict__ u, float* __restrict__ out, Geo G,
                                                                int N, const PdeBCRules Rl, Shell S) {
   GlobalAcc U{u, G.cstride[0], G.cstride[1], N};
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(256) heat_fill_ghosts_kernel(float* __restrict
     const float u2 = bc_eval(G, Rl, U, c[0], c[1], c[2], v);
     const long long k = ((long long)c[0] * G.n[1] + c[1]) * G.n[2] + c[2];
     u[k * N + v] = u2;
-    out[k * N + v] = u2;
+    if (out) out[k * N + v] = u2;
   }
 }
 

@@ -597,7 +597,8 @@ int heat3d_split_run(const float* u_in, float* u_out, float* work, const Geo& G,
       for (int i = 0; i < rules->ngroups; ++i)
         if (rules->group[i].func == PDE_BC_FUNC_RAMP)
           Rs.group[i].value = host_ramp_value(rules->group[i], t0, tstep, (long long)n0 + s);
-    heat_fill_ghosts_kernel<<<blocks_for(gs.off[6]), 256, 0, st>>>(src, dst, G, 1, Rs, gs);
+    heat_fill_ghosts_kernel<<<blocks_for(gs.off[6]), 256, 0, st>>>(src, (s == 0 || s == nsteps - 1) ? dst : nullptr,
+                                                                    G, 1, Rs, gs);
     heat_fill_nodes_kernel<<<blocks_for(ns.off[6]), 256, 0, st>>>(src, G, 1, Rs, ns);
     int rc = launch_status();
     if (rc) return rc;
