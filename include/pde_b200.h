@@ -259,7 +259,9 @@ int pde_heat_rollout_at(const float* u_in, float* u_out, float* work, const PdeG
 /* pde_heat_rollout_at continuing a run at step n0 >= 0: step n of the call
  * fills the boundary at fp32(t0 + (n0 + n) * t_step), so consecutive calls of
  * k steps (n0 = 0, k, 2k, ...) equal one call of the whole run bit for bit (the
- * slab rollout's blocks between halo exchanges). */
+ * slab rollout's blocks between halo exchanges).  u_in is scratch here: its
+ * contents may be overwritten (the one-step 3D path fills its boundary cells in
+ * place instead of copying it first). */
 int pde_heat_rollout_from(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
                           int32_t ncomp, const PdeBCRules* rules, float alpha, float dt,
                           int32_t nsteps, int32_t steps_per_pass, double t0, double t_step,

@@ -567,15 +567,20 @@ int heat_depth(const Geo& G, int ncomp, int steps_per_pass) {
 // and the OP_HEAT streaming kernel over the stencil box.  The caller's input is
 // first copied into a buffer of this call (the fill writes in place), chosen so
 // the last step lands in u_out; with u_out == u_in the rollout runs in place.
+// input_scratch: the caller lets the input be overwritten, so step 0 fills it
+// in place and the steps alternate between work and u_out, ending in u_out.
 int heat3d_split_run(const float* u_in, float* u_out, float* work, const Geo& G, const Weights& W,
                      const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, double t0, double tstep,
-                     int32_t n0, cudaStream_t st) {
+                     int32_t n0, bool input_scratch, cudaStream_t st) {
   const size_t bytes = (size_t)(G.n[0] * G.n[1] * G.n[2]) * sizeof(float);
   float* src;
   float* dst;
   if (u_out == u_in) {
     src = u_out;
     dst = work;
+  } else if (input_scratch) {
+    src = const_cast<float*>(u_in);
+    dst = (nsteps & 1) ? u_out : work;  // step s writes u_out when nsteps - 1 - s is even
   } else {
     float* first = (nsteps & 1) ? work : u_out;
     PDE_CUDA_CHECK(cudaMemcpyAsync(first, u_in, bytes, cudaMemcpyDeviceToDevice, st));
@@ -609,7 +614,7 @@ int heat3d_split_run(const float* u_in, float* u_out, float* work, const Geo& G,
     if (rc) return rc;
     float* t = src;
     src = dst;
-    dst = t;
+    dst = (input_scratch && t == u_in) ? (src == u_out ? work : u_out) : t;  // u_in only as the first source
   }
   if (src != u_out) PDE_CUDA_CHECK(cudaMemcpyAsync(u_out, src, bytes, cudaMemcpyDeviceToDevice, st));
   return PDE_OK;
@@ -619,7 +624,7 @@ int heat3d_split_run(const float* u_in, float* u_out, float* work, const Geo& G,
 // the call fills the boundary at fp32(t0 + (n0 + n) * tstep).
 int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid* grid, int32_t ncomp,
                      const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
-                     bool allow_ramp, double t0, double tstep, int32_t n0, void* stream) {
+                     bool allow_ramp, double t0, double tstep, int32_t n0, void* stream, bool input_scratch = false) {
   if (!u_in || !u_out || !work || !grid || !rules || nsteps < 0 || steps_per_pass < 0 || n0 < 0) return PDE_ERR_ARG;
   if (ncomp < 1 || ncomp > PDE_FUSED_MAX_COMP || rules->ncomp != ncomp) return PDE_ERR_ARG;
   if (rules->has_ramp && !allow_ramp) return PDE_ERR_UNSUPPORTED;
@@ -641,7 +646,7 @@ int heat_rollout_run(const float* u_in, float* u_out, float* work, const PdeGrid
   int k = heat_depth(G, ncomp, steps_per_pass);
   if (k > nsteps) k = nsteps;
   if (s3d && k == 1 && heat_split_shape(G, ncomp) && aligned16(u_in) && aligned16(u_out) && aligned16(work))
-    return heat3d_split_run(u_in, u_out, work, G, W, rules, alpha, dt, nsteps, t0, tstep, n0, st);
+    return heat3d_split_run(u_in, u_out, work, G, W, rules, alpha, dt, nsteps, t0, tstep, n0, input_scratch, st);
   const int npasses = (nsteps + k - 1) / k;
   // buffer sequence: the last pass writes u_out.
   const float* src = u_in;
@@ -772,7 +777,7 @@ int pde_heat_rollout_from(const float* u_in, float* u_out, float* work, const Pd
                           const PdeBCRules* rules, float alpha, float dt, int32_t nsteps, int32_t steps_per_pass,
                           double t0, double t_step, int32_t n0, void* stream) {
   return heat_rollout_run(u_in, u_out, work, grid, ncomp, rules, alpha, dt, nsteps, steps_per_pass, true, t0, t_step,
-                          n0, stream);
+                          n0, stream, true);
 }
 
 int pde_heat_pass_depth(const PdeGrid* grid, int32_t ncomp, int32_t steps_per_pass) {
