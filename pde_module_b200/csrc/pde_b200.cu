@@ -1121,8 +1121,12 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
   const int tiles = ((Pa.X + Pa.TBX - 1) / Pa.TBX) * Pa.tiles_y;
   const int threads = pick_threads_2d(tiles);
   const int cpt = wave_cells_per_thread(Pa.RC, threads);
-  auto kern = cpt == 4 ? wave_pair_tb_kernel<4> : cpt == 6 ? wave_pair_tb_kernel<6> : cpt == 8 ? wave_pair_tb_kernel<8> : wave_pair_tb_kernel<0>;
-  PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // register lists: the packed kernel (two cells per slot, cpt/2 slots); beyond 8
+  // cells per thread the general loop
+  auto kern = cpt == 4 ? wave_pair2_tb_kernel<2> : cpt == 6 ? wave_pair2_tb_kernel<3> : wave_pair2_tb_kernel<4>;
+  auto kern0 = wave_pair_tb_kernel<0>;
+  if (cpt > 0) PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  else PDE_CUDA_CHECK(cudaFuncSetAttribute(kern0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   float* w[6];
   for (int i = 0; i < 6; ++i) w[i] = work + (size_t)i * Pa.cells;
   // forward part: (u_prev, u_cur) -> (w0, w1) -> (w2, w3) -> (w0, w1) ...; the inputs are never written
@@ -1145,7 +1149,8 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
     float* fo_b = w[2 * fslot + 1];
     float* mo_a = to_out ? mu_out : w[4];
     float* mo_b = to_out ? mu_out_next : w[5];
-    kern<<<tiles, threads, smem, st>>>(fa, fb, fo_a, fo_b, ma, mb, mo_a, mo_b, K, Pf, Pa);
+    if (cpt > 0) kern<<<tiles, threads, smem, st>>>(fa, fb, fo_a, fo_b, ma, mb, mo_a, mo_b, K, Pf, Pa, -0.0f);
+    else kern0<<<tiles, threads, smem, st>>>(fa, fb, fo_a, fo_b, ma, mb, mo_a, mo_b, K, Pf, Pa);
     const int rc = launch_status();
     if (rc) return rc;
     if (Pf.k > 0) {

@@ -539,4 +539,193 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
   });
 }
 
+// ---- paired launch, packed: two cells per register slot --------------------
+// wave_pair_tb_kernel's register-list path with each slot holding two cells of
+// the rectangle walked at full region width: warp w's slot c covers the 64
+// consecutive cells from 64 (w + c W) (W warps), lane l taking cells l and
+// l + 32 of them, so each half of a slot reads 32 consecutive cells (odd
+// NB-float stride: no bank conflicts).  Both chains' arithmetic runs as packed
+// pairs -- each product __ffma2_rn with a run-time -0 addend (the exactly
+// rounded product), each sum __fadd2_rn, a - b as a + (-b) -- so each half is
+// the scalar kernel's operation sequence and the results are bit-identical to
+// it.  A half outside the rectangle computes on an in-region cell (its own, or
+// the first rectangle cell past the last row) and stores nothing.
+template <int MAXP>
+struct WavePairs {
+  int ri[MAXP][2];    // region index (always inside the region)
+  int gi[MAXP][2];    // array index of a tile cell; 0 (a valid address) for the other cells
+  int dist[MAXP][2];  // distance from the tile; 1 << 20 for a half outside the rectangle
+  unsigned tile;      // bit 2c + h: half h of slot c holds a tile cell
+  __device__ bool is_tile(int c, int h) const { return (tile >> (2 * c + h)) & 1u; }
+  __device__ WavePairs(const WaveRect& Rt, const WaveRegion& Rg, int Y) {
+    const int nw = (int)blockDim.x >> 5, w = (int)threadIdx.x >> 5, lane = (int)threadIdx.x & 31;
+    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0;
+    const int n = Rt.NR * Rg.RY;
+    const int ri_safe = Rt.cx0 * Rg.RY + Rt.cy0;  // a rectangle cell: every neighbour inside the region
+    tile = 0;
+#pragma unroll
+    for (int c = 0; c < MAXP; ++c) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int q = 64 * (w + c * nw) + lane + 32 * h;  // cell of the walk: row q / RY, region column q % RY
+        ri[c][h] = ri_safe;
+        gi[c][h] = 0;
+        dist[c][h] = 1 << 20;
+        if (q < n) {
+          const int row = q / Rg.RY, col = q - row * Rg.RY;
+          ri[c][h] = (Rt.cx0 + row) * Rg.RY + col;  // rows cx0 .. cx0+NR-1: neighbours inside the region
+          if (col >= Rt.cy0 && col < Rt.cy0 + Rt.W) {
+            const int ox = row - tx0, oy = col - ty0;
+            if (ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY) {
+              gi[c][h] = (Rg.bx0 + ox) * Y + Rg.by0 + oy;
+              tile |= 1u << (2 * c + h);
+            }
+            dist[c][h] = max(max(max(-ox, ox - (Rg.OX - 1)), max(-oy, oy - (Rg.OY - 1))), 0);
+          }
+        }
+      }
+    }
+  }
+};
+
+__device__ __forceinline__ float2 wv_neg(float2 a) { return make_float2(-a.x, -a.y); }
+
+template <int MAXP>
+__global__ void __launch_bounds__(1024) wave_pair2_tb_kernel(const float* __restrict__ um_in,
+                                                              const float* __restrict__ u0_in,
+                                                              float* __restrict__ um_out, float* __restrict__ u0_out,
+                                                              const float* __restrict__ m1_in,
+                                                              const float* __restrict__ m2_in,
+                                                              float* __restrict__ m1_out, float* __restrict__ m2_out,
+                                                              const float* __restrict__ Kf, const WaveParams Pf,
+                                                              const WaveParams Pa, const float negzero) {
+  extern __shared__ __align__(16) float sm[];
+  constexpr int NB = 7;
+  const int H = max(Pf.k, Pa.k);
+  const WaveRegion Rg(Pa, H);
+  const int RY = Rg.RY, rs = NB * RY;
+  const bool fwd = Pf.k > 0, adj = Pa.k > 0;
+  for_region(Rg, [&](int i, int x, int y) {
+    const size_t gi = (size_t)x * Pa.Y + y;
+    const bool in = wave_inside(Pa, x, y);
+    float* pc = sm + NB * i;
+    cp_async4(pc + 6, Kf + gi, true);
+    if (fwd) {
+      cp_async4(pc, um_in + gi, in);
+      cp_async4(pc + 1, u0_in + gi, in);
+    }
+    if (adj) {
+      cp_async4(pc + 2, m2_in + gi, in);
+      cp_async4(pc + 3, m1_in + gi, in);
+      pc[4] = 0.0f;
+    }
+  });
+  cp_async_wait_all();
+  if (adj) for_region(Rg, [&](int i, int x, int y) { sm[NB * i + 5] = mul(sm[NB * i + 6], sm[NB * i + 3]); });
+  __syncthreads();
+  const WaveRect Rt(Pa, Rg);
+  const int srci = wave_src_index(Pf, Rg);
+  const WavePairs<MAXP> C(Rt, Rg, Pa.Y);
+  const float2 nz2 = make_float2(negzero, negzero), two2 = make_float2(2.0f, 2.0f), zero2 = make_float2(0.0f, 0.0f);
+  auto M2 = [&](float2 a, float2 b) { return __ffma2_rn(a, b, nz2); };
+  float2 wf[3], wa[3];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    wf[t] = make_float2(Pf.w[t], Pf.w[t]);
+    wa[t] = make_float2(Pa.w[t], Pa.w[t]);
+  }
+  // the reference's 5-point sum (lap5n): x taps low to high, then y taps, from 0
+  auto lap2 = [&](const float* p0, const float* p1, const float2 (&w)[3]) {
+    auto ld = [&](int o) { return make_float2(p0[o], p1[o]); };
+    float2 acc = __fadd2_rn(zero2, M2(w[0], ld(-rs)));
+    acc = __fadd2_rn(acc, M2(w[1], ld(0)));
+    acc = __fadd2_rn(acc, M2(w[2], ld(rs)));
+    acc = __fadd2_rn(acc, M2(w[0], ld(-NB)));
+    acc = __fadd2_rn(acc, M2(w[1], ld(0)));
+    return __fadd2_rn(acc, M2(w[2], ld(NB)));
+  };
+  float2 ga[MAXP], lv[MAXP], kc[MAXP];
+#pragma unroll
+  for (int c = 0; c < MAXP; ++c) {
+    ga[c] = zero2;
+    lv[c] = zero2;
+    kc[c] = make_float2(sm[NB * C.ri[c][0] + 6], sm[NB * C.ri[c][1] + 6]);
+    if (adj) {
+      const float* L0 = Pa.lsts + (size_t)Pa.ntop * Pa.cells;
+      ga[c] = make_float2(C.is_tile(c, 0) ? Pa.gK[C.gi[c][0]] : 0.0f, C.is_tile(c, 1) ? Pa.gK[C.gi[c][1]] : 0.0f);
+      lv[c] = make_float2(__ldg(L0 + C.gi[c][0]), __ldg(L0 + C.gi[c][1]));
+    }
+  }
+  auto step = [&](auto PAR, int s) {
+    constexpr int p = decltype(PAR)::value;
+    const bool fs = s < Pf.k;
+    const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
+    float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
+    const int freach = Pf.k - 1 - s, areach = Pa.k - 1 - s;  // negative past a chain's last step
+#pragma unroll
+    for (int c = 0; c < MAXP; ++c) {
+      float* p0 = sm + NB * C.ri[c][0];
+      float* p1 = sm + NB * C.ri[c][1];
+      const bool f0 = C.dist[c][0] <= freach, f1 = C.dist[c][1] <= freach;
+      if (f0 || f1) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+        const float2 lap = lap2(p0 + (1 - p), p1 + (1 - p), wf);
+        float2 v = __fadd2_rn(M2(two2, make_float2(p0[1 - p], p1[1 - p])), wv_neg(make_float2(p0[p], p1[p])));
+        v = __fadd2_rn(v, M2(kc[c], lap));
+        if (C.ri[c][0] == srci) v.x = add(v.x, sn);
+        if (C.ri[c][1] == srci) v.y = add(v.y, sn);
+        if (f0) p0[p] = v.x;
+        if (f1) p1[p] = v.y;
+        st_global_if(Ls + C.gi[c][0], lap.x, f0 && C.is_tile(c, 0));
+        st_global_if(Ls + C.gi[c][1], lap.y, f1 && C.is_tile(c, 1));
+      }
+      const bool a0 = C.dist[c][0] <= areach, a1 = C.dist[c][1] <= areach;
+      if (a0 || a1) {  // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1}); dJ/dK += mu^{n+1} o L(u^n)
+        const float2 m1 = make_float2(p0[3 - p], p1[3 - p]);
+        ga[c] = __fadd2_rn(ga[c], M2(m1, lv[c]));  // a tile half is always in reach: no other half's sum is kept
+        const float2 acc = lap2(p0 + (5 - p), p1 + (5 - p), wa);
+        const float2 v =
+            __fadd2_rn(__fadd2_rn(M2(two2, m1), wv_neg(make_float2(p0[2 + p], p1[2 + p]))), acc);
+        const float2 km = M2(kc[c], v);
+        if (a0) {
+          p0[2 + p] = v.x;
+          p0[4 + p] = km.x;
+        }
+        if (a1) {
+          p1[2 + p] = v.y;
+          p1[4 + p] = km.y;
+        }
+      }
+    }
+    if (s + 1 < Pa.k) {  // the next step's L(u^n), in flight across the barrier
+      const float* L1 = Pa.lsts + (size_t)(Pa.ntop - s - 1) * Pa.cells;
+#pragma unroll
+      for (int c = 0; c < MAXP; ++c) lv[c] = make_float2(__ldg(L1 + C.gi[c][0]), __ldg(L1 + C.gi[c][1]));
+    }
+    __syncthreads();
+  };
+  for (int s = 0; s < H; s += 2) {
+    step(IC<0>{}, s);
+    if (s + 1 < H) step(IC<1>{}, s + 1);
+  }
+  if (adj) {
+#pragma unroll
+    for (int c = 0; c < MAXP; ++c) {
+      if (C.is_tile(c, 0)) Pa.gK[C.gi[c][0]] = ga[c].x;
+      if (C.is_tile(c, 1)) Pa.gK[C.gi[c][1]] = ga[c].y;
+    }
+  }
+  const int fw = (Pf.k & 1) ? 0 : 1, aw = (Pa.k & 1) ? 0 : 1;  // levels the last steps wrote
+  for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) {
+    const float* pc = sm + NB * ri;
+    if (fwd) {
+      um_out[gi] = pc[1 - fw];
+      u0_out[gi] = pc[fw];
+    }
+    if (adj) {
+      m1_out[gi] = pc[2 + aw];
+      m2_out[gi] = pc[3 - aw];
+    }
+  });
+}
+
 }  // namespace pde
