@@ -358,8 +358,9 @@ int pde_grad_ex(const float* in, float* out, const PdeGrid* grid, int32_t ncomp,
   const Weights W = d1_weights(G.order, grid->dx);
   cudaStream_t st = as_stream(stream);
   if (ncomp == 1 && stream3d_ok(in, G, 1)) {
-    if (G.order == 2) return launch_selected<1, OP_GRAD, 1, 64, 32, 8, 4>(S3K_GRAD, in, out, G, W, alpha, mode, st);
-    return launch_selected<2, OP_GRAD, 1, 64, 32, 8, 4>(S3K_GRAD, in, out, G, W, alpha, mode, st);
+    // default tile (fast mode, and shapes without the double-row map): 128 x 8, 4 rows per thread
+    if (G.order == 2) return launch_selected<1, OP_GRAD, 1, 128, 8, 4, 4>(S3K_GRAD, in, out, G, W, alpha, mode, st);
+    return launch_selected<2, OP_GRAD, 1, 128, 8, 4, 4>(S3K_GRAD, in, out, G, W, alpha, mode, st);
   }
   const int64_t total = G.ext[0] * G.ext[1] * G.ext[2] * ncomp * G.ndims;
   const int blocks = grid_blocks(total, 256);
