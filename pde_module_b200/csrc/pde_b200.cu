@@ -1128,7 +1128,7 @@ int pde_wave_pair(const float* K, const float* u_prev, const float* u_cur, int32
   // register lists: the packed kernel (two cells per slot, cpt/2 slots); beyond 8
   // cells per thread the general loop
   auto kern = cpt == 4 ? wave_pair2_tb_kernel<2> : cpt == 6 ? wave_pair2_tb_kernel<3> : wave_pair2_tb_kernel<4>;
-  auto kern0 = wave_pair_tb_kernel<0>;
+  auto kern0 = wave_pair_tb_kernel;
   if (cpt > 0) PDE_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   else PDE_CUDA_CHECK(cudaFuncSetAttribute(kern0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   float* w[6];

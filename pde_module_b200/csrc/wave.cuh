@@ -386,9 +386,9 @@ __global__ void __launch_bounds__(1024) wave_adj_tb_kernel(const float* __restri
 // are independent, so each warp interleaves two dependency chains and a step
 // of both costs one barrier.  Arithmetic and per-cell operation order are
 // those of the two kernels above.  Shared memory: the NB = 7 interleaved
-// region, then the gradient tile (MAXC = 0).  MAXC as in wave_adj_tb_kernel
-// (the forward's stored Laplacians use the same tile indices).
-template <int MAXC>
+// region, then the gradient tile.  This is the general loop over the
+// rectangle (any region size); rectangles of up to 8 cells per thread run
+// the packed register-list kernel below.
 __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restrict__ um_in,
                                                              const float* __restrict__ u0_in,
                                                              float* __restrict__ um_out, float* __restrict__ u0_out,
@@ -419,112 +419,50 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
       pc[4] = 0.0f;
     }
   });
-  if (adj && MAXC == 0)
-    for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, Pa.gK + gi, true); });
+  if (adj) for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { cp_async4(sm + oga + t, Pa.gK + gi, true); });
   cp_async_wait_all();
   if (adj) for_region(Rg, [&](int i, int x, int y) { sm[NB * i + 5] = mul(sm[NB * i + 6], sm[NB * i + 3]); });
   __syncthreads();
   const WaveRect Rt(Pa, Rg);
   const int srci = wave_src_index(Pf, Rg);
-  if constexpr (MAXC > 0) {
-    const WaveCells<MAXC> C(Rt, Rg, Pa.Y);
-    // lv as in wave_adj_tb_kernel; the forward's Laplacians are stored with a
-    // predicated store (tile cells only)
-    float ga[MAXC], lv[MAXC], kc[MAXC];
-#pragma unroll
-    for (int c = 0; c < MAXC; ++c) {
-      ga[c] = 0.0f;
-      lv[c] = 0.0f;
-      kc[c] = C.ri[c] >= 0 ? sm[NB * C.ri[c] + 6] : 0.0f;  // K of the thread's cells, for both chains
-      if (adj) {
-        if (C.is_tile(c)) ga[c] = Pa.gK[C.gi[c]];
-        lv[c] = __ldg(Pa.lsts + (size_t)Pa.ntop * Pa.cells + C.gi[c]);
+  const int nt = (int)blockDim.x;
+  const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
+  for (int s = 0; s < H; ++s) {
+    const int p = s & 1;
+    const bool fs = s < Pf.k, as = s < Pa.k;
+    const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
+    float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
+    const float* Ln = as ? Pa.lsts + (size_t)(Pa.ntop - s) * Pa.cells : nullptr;
+    RectWalk wk(Rt.W, nt);
+    for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
+      const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
+      float* pc = sm + NB * i;
+      const int ox = wk.row - tx0, oy = wk.col - ty0;
+      const bool tile = ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY;
+      if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
+        const float lap = lap5n<NB>(pc + (1 - p), rs, Pf.w);
+        float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
+        v = add(v, mul(pc[6], lap));
+        if (i == srci) v = add(v, sn);
+        pc[p] = v;
+        if (tile) Ls[(size_t)(Rg.bx0 + ox) * Pf.Y + Rg.by0 + oy] = lap;
+      }
+      if (as) {
+        const float m1 = pc[3 - p];
+        if (tile) {  // dJ/dK += mu^{n+1} o L(u^n)
+          const int t = oga + ox * Rg.OY + oy;
+          sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * Pa.Y + Rg.by0 + oy)));
+        }
+        // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
+        const float acc = lap5n<NB>(pc + (5 - p), rs, Pa.w);
+        const float v = add(sub(mul(2.0f, m1), pc[2 + p]), acc);
+        pc[2 + p] = v;
+        pc[4 + p] = mul(pc[6], v);
       }
     }
-    auto step = [&](auto PAR, int s) {
-      constexpr int p = decltype(PAR)::value;
-      const bool fs = s < Pf.k;
-      const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
-      float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
-      // a chain past its last step has a negative reach (dist >= 0)
-      const int freach = Pf.k - 1 - s, areach = Pa.k - 1 - s;
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c) {
-        float* pc = sm + NB * C.ri[c];
-        if (C.dist[c] <= freach) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
-          const float lap = lap5n<NB>(pc + (1 - p), rs, Pf.w);
-          float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
-          v = add(v, mul(kc[c], lap));
-          if (C.ri[c] == srci) v = add(v, sn);
-          pc[p] = v;
-          st_global_if(Ls + C.gi[c], lap, C.is_tile(c));
-        }
-        if (C.dist[c] <= areach) {
-          const float m1 = pc[3 - p];
-          ga[c] = add(ga[c], mul(m1, lv[c]));  // dJ/dK += mu^{n+1} o L(u^n) (kept for tile cells)
-          // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
-          const float acc = lap5n<NB>(pc + (5 - p), rs, Pa.w);
-          const float v = add(sub(mul(2.0f, m1), pc[2 + p]), acc);
-          pc[2 + p] = v;
-          pc[4 + p] = mul(kc[c], v);
-        }
-      }
-      if (s + 1 < Pa.k) {  // the next step's L(u^n), in flight across the barrier
-        const float* L1 = Pa.lsts + (size_t)(Pa.ntop - s - 1) * Pa.cells;
-#pragma unroll
-        for (int c = 0; c < MAXC; ++c) lv[c] = __ldg(L1 + C.gi[c]);
-      }
-      __syncthreads();
-    };
-    for (int s = 0; s < H; s += 2) {
-      step(IC<0>{}, s);
-      if (s + 1 < H) step(IC<1>{}, s + 1);
-    }
-    if (adj) {
-#pragma unroll
-      for (int c = 0; c < MAXC; ++c)
-        if (C.is_tile(c)) Pa.gK[C.gi[c]] = ga[c];
-    }
-  } else {
-    const int nt = (int)blockDim.x;
-    const int tx0 = Rg.bx0 - Rg.rx0 - Rt.cx0, ty0 = Rg.by0 - Rg.ry0 - Rt.cy0;
-    for (int s = 0; s < H; ++s) {
-      const int p = s & 1;
-      const bool fs = s < Pf.k, as = s < Pa.k;
-      const float sn = (fs && srci >= 0) ? Pf.src[Pf.n0 + s] : 0.0f;
-      float* Ls = fs ? Pf.lst + (size_t)s * Pf.cells : nullptr;
-      const float* Ln = as ? Pa.lsts + (size_t)(Pa.ntop - s) * Pa.cells : nullptr;
-      RectWalk wk(Rt.W, nt);
-      for (int q = threadIdx.x; q < Rt.count; q += nt, wk.next()) {
-        const int i = (Rt.cx0 + wk.row) * RY + Rt.cy0 + wk.col;
-        float* pc = sm + NB * i;
-        const int ox = wk.row - tx0, oy = wk.col - ty0;
-        const bool tile = ox >= 0 && ox < Rg.OX && oy >= 0 && oy < Rg.OY;
-        if (fs) {  // u^{n+1} = 2 u^n - u^{n-1} + K o L(u^n) (+ source)
-          const float lap = lap5n<NB>(pc + (1 - p), rs, Pf.w);
-          float v = sub(mul(2.0f, pc[1 - p]), pc[p]);
-          v = add(v, mul(pc[6], lap));
-          if (i == srci) v = add(v, sn);
-          pc[p] = v;
-          if (tile) Ls[(size_t)(Rg.bx0 + ox) * Pf.Y + Rg.by0 + oy] = lap;
-        }
-        if (as) {
-          const float m1 = pc[3 - p];
-          if (tile) {  // dJ/dK += mu^{n+1} o L(u^n)
-            const int t = oga + ox * Rg.OY + oy;
-            sm[t] = add(sm[t], mul(m1, __ldg(Ln + (size_t)(Rg.bx0 + ox) * Pa.Y + Rg.by0 + oy)));
-          }
-          // mu^n = 2 mu^{n+1} - mu^{n+2} + L(K o mu^{n+1})
-          const float acc = lap5n<NB>(pc + (5 - p), rs, Pa.w);
-          const float v = add(sub(mul(2.0f, m1), pc[2 + p]), acc);
-          pc[2 + p] = v;
-          pc[4 + p] = mul(pc[6], v);
-        }
-      }
-      __syncthreads();
-    }
-    if (adj) for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { Pa.gK[gi] = sm[oga + t]; });
+    __syncthreads();
   }
+  if (adj) for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) { Pa.gK[gi] = sm[oga + t]; });
   const int fw = (Pf.k & 1) ? 0 : 1, aw = (Pa.k & 1) ? 0 : 1;  // levels the last steps wrote
   for_tile(Rg, Pa.Y, [&](int t, int ri, size_t gi) {
     const float* pc = sm + NB * ri;
@@ -540,7 +478,7 @@ __global__ void __launch_bounds__(1024) wave_pair_tb_kernel(const float* __restr
 }
 
 // ---- paired launch, packed: two cells per register slot --------------------
-// wave_pair_tb_kernel's register-list path with each slot holding two cells of
+// The paired launch's register-list form, each slot holding two cells of
 // the rectangle walked at full region width: warp w's slot c covers the 64
 // consecutive cells from 64 (w + c W) (W warps), lane l taking cells l and
 // l + 32 of them, so each half of a slot reads 32 consecutive cells (odd

@@ -86,10 +86,24 @@ def test_autograd_speed_gradient_matches_float64():
     assert relu < 1e-3
 
 
-@pytest.mark.parametrize("nf,na,k", [(7, 5, 3), (9, 9, 4), (0, 6, 4), (5, 0, 2), (12, 3, 16)])
-def test_pair_equals_separate_calls(nf, na, k):
+@pytest.mark.parametrize("nf,na,k,launch", [(7, 5, 3, None), (9, 9, 4, None), (0, 6, 4, None), (5, 0, 2, None),
+                                             (12, 3, 16, None), (7, 5, 3, (48, 48, 256)), (9, 9, 4, (48, 48, 256))])
+def test_pair_equals_separate_calls(nf, na, k, launch):
     """pde_wave_pair (forward recomputation of one segment beside the adjoint of
-    another) is bit-identical to pde_wave_forward + pde_wave_adjoint."""
+    another) is bit-identical to pde_wave_forward + pde_wave_adjoint: the packed
+    register-list kernel, and with 48x48 tiles of 256 threads (more than 8
+    rectangle cells per thread) the general loop."""
+    import ctypes as C
+    from pde_module_b200 import _lib
+    if launch is not None:
+        _lib.check(_lib.lib().pde_set_launch_2d(*launch), "pde_set_launch_2d")
+    try:
+        _pair_vs_separate(nf, na, k)
+    finally:
+        _lib.lib().pde_set_launch_2d(0, 0, 0)
+
+
+def _pair_vs_separate(nf, na, k):
     import ctypes as C
     from pde_module_b200 import _lib
     K, u0, src, cell, N, dx, _, _ = _setup(X=70, Y=90, N=20)
