@@ -235,8 +235,13 @@ int pde_bc_compile(const PdeBCGroup* groups, int32_t ngroups, const PdeGrid* gri
  * steps_per_pass: temporal-blocking depth k (0 = choose).  2D (Z == 1) grids use
  * shared-memory tiles with k steps per pass.  3D grids whose interior has at
  * least 3 cells per axis stream along X with k steps per pass (k at most 4 for
- * one component, 2 for more; deeper requests run at that depth; 0 chooses 2 for
- * order 2 and 1 for order 4); smaller 3D grids take one step per pass.
+ * one component, 2 for more; deeper requests run at that depth).  At k = 1 a
+ * scalar field whose shape takes the double-row map (even Y and Z, plane pitch
+ * a multiple of 4 floats, even g - R) runs a surface fill and the TMA streaming
+ * heat step per step, and 0 chooses k = 1 there; otherwise 0 chooses 2 for
+ * order 2 and 1 for order 4 (pde_heat_pass_depth).  Smaller 3D grids take one
+ * step per pass.  The input is never written (the streaming path copies it once
+ * into a buffer of the call unless u_out == u_in).
  * Constant-valued groups only: rules with a ramp group (has_ramp) give
  * PDE_ERR_UNSUPPORTED here; pde_heat_rollout_at takes them. */
 int pde_heat_rollout(const float* u_in, float* u_out, float* work, const PdeGrid* grid,
