@@ -278,3 +278,42 @@ def test_local_slabs_equal_single_array(world, order, k):
             slabs[0](1)
         else:
             raise RuntimeError
+
+
+def _lost_rank_worker(rank, world, port, q):
+    """Rank 1 leaves before the exchange; rank 0's exchange must end with an error
+    (the peer's connection closes, or the 10 s process-group timeout runs out)."""
+    import time
+    from datetime import timedelta
+    from pde_module_b200.distributed import exchange_cut_planes
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=10))
+    if rank == 1:
+        q.put((1, "left"))
+        q.close()
+        q.join_thread()  # the message is out before the process goes
+        os._exit(0)  # gone without a goodbye: no destroy_process_group
+    field = torch.zeros((4 + 3, 5, 6, 1))
+    t0 = time.time()
+    try:
+        exchange_cut_planes(field, 0, 4, 3)
+        q.put((0, "no error"))
+    except Exception as e:  # the lost peer is reported, not waited on forever
+        q.put((0, f"error after {time.time() - t0:.1f} s: {type(e).__name__}"))
+
+
+def test_slab_exchange_reports_a_lost_rank():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_lost_rank_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in ps:
+        p.join(timeout=30)
+        if p.is_alive():
+            p.kill()
+    assert res[1] == "left"
+    assert res[0].startswith("error after"), res[0]
