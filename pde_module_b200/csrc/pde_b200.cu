@@ -177,7 +177,7 @@ int launch_stream3d(const float* in, float* out, const Geo& G, const Weights& Wt
 // lane), so their tiles hold twice the z cells per lane of the others.
 enum { S3K_LAP1 = 0, S3K_LAP3 = 1, S3K_GRAD = 2, S3K_DIV = 3, S3K_KINDS = 4 };
 // Defaults [kind][order 2, order 4]: the fastest candidates of a sweep at 512^3 on B200.
-int g_s3_sel[S3K_KINDS][2] = {{2, 1}, {3, 3}, {3, 1}, {1, 1}};
+int g_s3_sel[S3K_KINDS][2] = {{2, 1}, {3, 3}, {1, 1}, {1, 1}};
 constexpr int kS3Candidates = 4;
 
 template <int R, int OP, int CIN>
@@ -212,7 +212,7 @@ int launch_candidate(int cand, const float* in, float* out, const Geo& G, const 
     }
   } else if constexpr (OP == OP_GRAD) {
     switch (cand) {
-      case 1: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
+      case 1: return launch_stream3d_k<R, OP, 1, 128, 16, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 2: return launch_stream3d_k<R, OP, 1, 128, 8, 4, 6, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       case 3: return launch_stream3d_k<R, OP, 1, 128, 8, 4, 4, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);
       default: return launch_stream3d_k<R, OP, 1, 64, 16, 4, 6, MAP_PAIRS, MODE_EXACT>(in, out, G, W, alpha, alpha, st);

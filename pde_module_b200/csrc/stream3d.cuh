@@ -338,13 +338,16 @@ __device__ __forceinline__ void s3_zpairs(const S3Params& P, float* smem, uint64
   if constexpr (OP == OP_GRAD) bulk_wait();  // this lane's bulk stores are done before the block exits
 }
 
+// Register budget: two resident blocks per SM up to 320 threads, one above
+// (a cap of two such blocks spilled at 56-72 registers).
 // Work items are (chunk of planes, tile) pairs in chunk-major order, dealt
 // round-robin to a persistent grid: the items in flight at any time share a
 // plane range, so neighbouring tiles read each other's halo rows from L2.
 // The stage ring and its barrier phases continue from one item to the next
 // (running stage counters), so the producer prefetches across items.
 template <int R, int OP, int CIN, int TZ, int TY, int YPT, int PREF, int MAPK, int MODE>
-__global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>::THREADS, 2)
+__global__ void __launch_bounds__(S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>::THREADS,
+                                   (S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>::THREADS > 320 ? 1 : 2))
     stream3d_kernel(const __grid_constant__ CUtensorMap tmap, const S3Params P, const FastW FW) {
   using C = S3Cfg<R, OP, CIN, TZ, TY, YPT, PREF, MAPK, MODE>;
   constexpr bool PP0 = (MAPK != MAP_ROWS_GEN);
